@@ -1,0 +1,69 @@
+// Internal definitions shared by the library's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "diskann_b200.h"
+
+// Device-resident in-memory index.  HBM layout:
+//  * vectors  : (N+F) rows x vstride floats, vstride = round_up(D, 4), rows 16-B aligned and
+//               zero padded, so a row is read with 16-byte loads;
+//  * adjacency: (N+F) rows x astride u32, row = [degree, id_0 .. id_{max_degree-1}, pad],
+//               astride = round_up(1 + max_degree, 4): one hop reads one contiguous row;
+//  * pq codes : (N+F) rows x cstride bytes, cstride = round_up(M, 16);
+//  * pq pivots: 256 x D floats (row-major, the FixedChunkPQTable layout); offsets: M+1 u32.
+struct dk_index {
+  int device = 0;
+  uint32_t n = 0, f = 0, dim = 0, max_degree = 0, pq_chunks = 0;
+  int32_t metric = 0;
+  uint32_t vstride = 0, astride = 0, cstride = 0;
+  float* vectors = nullptr;
+  uint32_t* adj = nullptr;
+  uint8_t* codes = nullptr;
+  float* pivots = nullptr;
+  uint32_t* offsets = nullptr;
+  uint64_t bytes = 0;
+};
+
+// Per-launch parameters of the beam-search kernels.
+struct SearchParams {
+  const float* vectors;
+  const uint32_t* adj;
+  const uint8_t* codes;
+  const float* pivots;
+  const uint32_t* offsets;
+  uint32_t n, f, dim, vstride, astride, max_degree, cstride, pq_chunks;
+  const float* queries;
+  uint64_t qstride;
+  uint32_t nq;
+  uint32_t k, l, cap, beam;
+  int32_t strategy;
+  uint32_t* out_ids;
+  float* out_dists;
+  dk_search_stats* stats;
+  // Visited set: shared-memory hash (first pass) or global bitmap slice per CTA (spill pass).
+  uint32_t hash_log2;
+  uint32_t hash_limit;  // inserts allowed before the hash counts as full
+  uint32_t* bitmap;
+  uint32_t bitmap_words;
+  // Shared-memory carve-up (byte offsets into dynamic shared memory).
+  uint32_t off_query, off_table, off_qd0, off_qi0, off_qd1, off_qi1;
+  uint32_t off_cand_id, off_cand_d, off_new_d, off_new_id, off_hash, off_misc;
+  uint32_t smem_bytes;
+  uint32_t list_cap;  // capacity of the candidate / rerank lists
+};
+
+constexpr uint32_t kFlagSpilled = 1u;
+
+// Thread-local error reporting for the C ABI.
+void dk_set_error(int32_t status, const std::string& msg);
+
+// Launch the search (first pass + spill pass) on `stream`.  Parameters are validated by
+// the caller.
+int32_t dk_launch_search(const dk_index* ix, int32_t strategy, const float* queries,
+                         uint64_t qstride, uint32_t nq, uint32_t k, uint32_t l, uint32_t beam,
+                         uint32_t* ids, float* dists, dk_search_stats* stats,
+                         cudaStream_t stream);

@@ -1,0 +1,248 @@
+"""Host-side mirror of the reference's search surface over the C ABI.
+
+Reference shapes mirrored here (paths relative to the reference repository):
+
+* ``Knn`` — diskann/src/graph/search/knn_search.rs:76-119 (k, L, beam width; validation and
+  the ``KnnSearchError`` kinds).
+* ``Metric`` — diskann-vector/src/distance/metric.rs:11-52 (same integer codes).
+* ``FullPrecision`` / ``Hybrid`` / ``Quantized`` — the in-memory strategies
+  (diskann-providers/.../inmem/full_precision.rs:476-506, inmem/product.rs:363-394, 537-566).
+* ``GpuProvider`` — the device-resident counterpart of ``DefaultProvider``
+  (inmem/provider.rs:227-352): vectors, optional PQ codes, fixed-slot adjacency and frozen
+  start points with ids ``num_points..num_points+F-1``.
+* ``DiskANNIndex.search`` — ``DiskANNIndex::search`` (diskann/src/graph/index.rs:2034-2070),
+  batched: it returns ids, distances and per-query ``SearchStats`` (index.rs:90-102).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import enum
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native
+
+STATS_DTYPE = np.dtype(
+    [("cmps", np.uint32), ("hops", np.uint32), ("result_count", np.uint32), ("flags", np.uint32)]
+)
+INVALID_ID = 0xFFFFFFFF
+
+
+class Metric(enum.IntEnum):
+    COSINE = 0
+    INNER_PRODUCT = 1
+    L2 = 2
+    COSINE_NORMALIZED = 3
+
+
+class Status(enum.IntEnum):
+    OK = 0
+    K_ZERO = 1
+    L_ZERO = 2
+    L_LESS_THAN_K = 3
+    BEAM_WIDTH_ZERO = 4
+    NO_PQ = 5
+    INVALID_ARGUMENT = 6
+    INVALID_GRAPH = 7
+    DIMENSION_MISMATCH = 8
+    OUT_OF_MEMORY = 9
+    CUDA = 10
+    DEVICE_TIMEOUT = 11
+    UNSUPPORTED = 12
+    ADMISSION = 13
+    CANCELLED = 14
+    NOT_FOUND = 15
+
+
+class ANNError(RuntimeError):
+    """An error returned by the C ABI (the reference's ``ANNError``)."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{Status(status).name}: {message}")
+        self.status = Status(status)
+        self.message = message
+
+
+class KnnSearchError(ANNError, ValueError):
+    """Invalid ``Knn`` parameters (knn_search.rs:39-44)."""
+
+
+def _check(status: int) -> None:
+    if status != 0:
+        st, msg = _native.last_error()
+        cls = KnnSearchError if status in (1, 2, 3, 4) else ANNError
+        raise cls(status, msg if st == status else "")
+
+
+class Knn:
+    """k-NN search parameters: ``Knn(k_value, l_value, beam_width=None)``."""
+
+    def __init__(self, k_value: int, l_value: int, beam_width: int | None = None):
+        bw = 1 if beam_width is None else int(beam_width)
+        if k_value == 0:
+            raise KnnSearchError(Status.K_ZERO, "k_value must be nonzero")
+        if l_value == 0:
+            raise KnnSearchError(Status.L_ZERO, "l_value must be nonzero")
+        if k_value > l_value:
+            raise KnnSearchError(
+                Status.L_LESS_THAN_K, f"l_value ({l_value}) cannot be less than k_value ({k_value})"
+            )
+        if bw == 0:
+            raise KnnSearchError(Status.BEAM_WIDTH_ZERO, "beam width must be nonzero")
+        self.k_value = int(k_value)
+        self.l_value = int(l_value)
+        self.beam_width = bw
+
+    def __repr__(self) -> str:
+        return f"Knn(k={self.k_value}, l={self.l_value}, beam_width={self.beam_width})"
+
+
+class _Strategy:
+    code = -1
+
+    def __repr__(self) -> str:
+        return type(self).__name__ + "()"
+
+
+class FullPrecision(_Strategy):
+    """FP32 traversal; FilterStartPoints + copy."""
+
+    code = 0
+
+
+class Hybrid(_Strategy):
+    """PQ (ADC) traversal; FilterStartPoints + exact full-precision Rerank."""
+
+    code = 1
+
+
+class Quantized(_Strategy):
+    """PQ (ADC) traversal; FilterStartPoints + copy."""
+
+    code = 2
+
+
+@dataclass
+class PQData:
+    """Product quantisation schema and codes (FixedChunkPQTable layout)."""
+
+    offsets: np.ndarray  # (M+1,) uint32
+    pivots: np.ndarray  # (256, D) float32
+    codes: np.ndarray  # (N+F, M) uint8
+
+
+class GpuProvider:
+    """Device-resident in-memory provider built from host arrays.
+
+    ``vectors`` (N+F, D) float32, ``adjacency`` (N+F, S) uint32 with ``degrees`` (N+F,);
+    rows ``num_points..`` are frozen start points.
+    """
+
+    def __init__(self, vectors, adjacency, degrees, num_points: int, metric=Metric.L2,
+                 pq: PQData | None = None, device: int = 0):
+        L = _native.load()
+        vectors = np.ascontiguousarray(vectors, dtype=np.float32)
+        adjacency = np.ascontiguousarray(adjacency, dtype=np.uint32)
+        degrees = np.ascontiguousarray(degrees, dtype=np.uint32)
+        d = _native.IndexDesc()
+        d.num_points = int(num_points)
+        d.num_frozen = vectors.shape[0] - int(num_points)
+        d.dim = vectors.shape[1]
+        d.metric = int(metric)
+        d.vectors = vectors.ctypes.data
+        d.vector_stride = vectors.shape[1]
+        d.adjacency = adjacency.ctypes.data
+        d.adjacency_stride = adjacency.shape[1]
+        d.degrees = degrees.ctypes.data
+        d.max_degree = adjacency.shape[1]
+        keep = [vectors, adjacency, degrees]
+        if pq is not None:
+            off = np.ascontiguousarray(pq.offsets, dtype=np.uint32)
+            piv = np.ascontiguousarray(pq.pivots, dtype=np.float32)
+            codes = np.ascontiguousarray(pq.codes, dtype=np.uint8)
+            d.pq_chunks = len(off) - 1
+            d.pq_offsets = off.ctypes.data
+            d.pq_pivots = piv.ctypes.data
+            d.pq_codes = codes.ctypes.data
+            d.pq_code_stride = codes.shape[1]
+            keep += [off, piv, codes]
+        handle = ctypes.c_void_p()
+        _check(L.dk_index_create(ctypes.byref(d), int(device), ctypes.byref(handle)))
+        del keep
+        self._handle = handle
+        self.num_points = int(num_points)
+        self.num_frozen = int(d.num_frozen)
+        self.dim = int(d.dim)
+        self.metric = Metric(int(metric))
+        self.device = int(device)
+        self.has_pq = pq is not None
+
+    @property
+    def handle(self):
+        if self._handle is None:
+            raise ANNError(Status.INVALID_ARGUMENT, "provider is closed")
+        return self._handle
+
+    def info(self) -> dict:
+        inf = _native.IndexInfo()
+        _check(_native.load().dk_index_get_info(self.handle, ctypes.byref(inf)))
+        return {f: getattr(inf, f) for f, _ in inf._fields_}
+
+    def close(self) -> None:
+        if getattr(self, "_handle", None) is not None:
+            _native.load().dk_index_destroy(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class DiskANNIndex:
+    """Graph index over a :class:`GpuProvider`; ``search`` runs batched greedy beam search."""
+
+    def __init__(self, provider: GpuProvider):
+        self.provider = provider
+
+    def search(self, params: Knn, strategy: _Strategy, queries):
+        """Search host queries (nq, D) float32; returns ``(ids, distances, stats)`` numpy arrays.
+
+        Host buffers cross the C ABI (``dk_search``): queries are copied to the device and
+        results back inside the call.
+        """
+        q = np.ascontiguousarray(np.atleast_2d(queries), dtype=np.float32)
+        if q.shape[1] != self.provider.dim:
+            raise ANNError(Status.DIMENSION_MISMATCH, f"query dim {q.shape[1]} != {self.provider.dim}")
+        nq, k = q.shape[0], params.k_value
+        ids = np.empty((nq, k), dtype=np.uint32)
+        dists = np.empty((nq, k), dtype=np.float32)
+        stats = np.zeros(nq, dtype=STATS_DTYPE)
+        _check(_native.load().dk_search(
+            self.provider.handle, strategy.code, q.ctypes.data, q.shape[1], nq, k,
+            params.l_value, params.beam_width, ids.ctypes.data, dists.ctypes.data, stats.ctypes.data,
+        ))
+        return ids, dists, stats
+
+    def search_device(self, params: Knn, strategy: _Strategy, queries, ids, dists, stats,
+                      stream=None) -> None:
+        """Search device-resident queries; outputs go to caller-allocated device buffers.
+
+        ``queries``: CUDA float32 tensor (nq, D); ``ids``: int32 (nq, k) (bit pattern of
+        uint32); ``dists``: float32 (nq, k); ``stats``: int32 (nq, 4).  Asynchronous on
+        ``stream`` (a torch.cuda.Stream or raw handle; default: torch's current stream).
+        """
+        import torch
+
+        if stream is None:
+            stream = torch.cuda.current_stream(queries.device)
+        handle = stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+        nq = queries.shape[0]
+        _check(_native.load().dk_search_device(
+            self.provider.handle, strategy.code, queries.data_ptr(), queries.stride(0), nq,
+            params.k_value, params.l_value, params.beam_width, ids.data_ptr(), dists.data_ptr(),
+            stats.data_ptr(), ctypes.c_void_p(handle),
+        ))

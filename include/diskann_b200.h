@@ -1,0 +1,153 @@
+/*
+ * diskann_b200 — C ABI of the B200 in-memory graph-search engine.
+ *
+ * This is the drop-in boundary for the reference's in-memory search call.  In the
+ * reference (a Rust workspace) a search is
+ *
+ *     DiskANNIndex::search(Knn::new(k, l, beam)?, &strategy, &ctx, query, &mut output)
+ *       diskann/src/graph/index.rs:2034-2070  ->  <Knn as Search>::search
+ *       diskann/src/graph/search/knn_search.rs:178-216
+ *
+ * run against an in-memory `DefaultProvider` (diskann-providers/src/model/graph/provider/
+ * async_/inmem/provider.rs:227-352) with one of the strategies `FullPrecision`
+ * (inmem/full_precision.rs:476-506), `Hybrid` (inmem/product.rs:363-394) or `Quantized`
+ * (inmem/product.rs:537-566).  The per-hop `SearchAccessor::expand_beam` callback
+ * (diskann/src/graph/glue.rs:125-254) is far too fine-grained to cross into a GPU, so the
+ * boundary sits at `Search::search` granularity and is batched: one call searches many
+ * queries.  The reference's own C FFI precedent is diskann-garnet/src/lib.rs:218-807
+ * (plain `extern "C"` functions over raw pointers and sizes, integer status codes).
+ *
+ * Conventions
+ *  - Every function returns an int32_t status (DK_OK == 0).  `dk_last_error` gives the
+ *    calling thread's last error message.
+ *  - Ids 0..num_points-1 are data points; ids num_points..num_points+num_frozen-1 are the
+ *    frozen start points (inmem/provider.rs:312-319), which are searched from and filtered
+ *    out of results (diskann/src/graph/glue.rs:730-773 FilterStartPoints).
+ *  - Output buffers are caller-allocated, k entries per query (the reference's
+ *    caller-allocated `SearchOutputBuffer`, diskann/src/graph/search_output_buffer.rs:100-140).
+ *    Entries past a query's result_count are id 0xFFFFFFFF, distance +inf.
+ *  - Thread safety: create/destroy are exclusive; search calls on one index are safe from
+ *    several host threads and streams at once (the index is read-only after creation).
+ */
+#ifndef DISKANN_B200_H
+#define DISKANN_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DK_ABI_VERSION 1
+#define DK_INVALID_ID 0xFFFFFFFFu
+
+/* Metric codes are the reference's i32 encoding (diskann-vector/src/distance/metric.rs:34-52). */
+enum dk_metric {
+  DK_METRIC_COSINE = 0,
+  DK_METRIC_INNER_PRODUCT = 1,
+  DK_METRIC_L2 = 2,
+  DK_METRIC_COSINE_NORMALIZED = 3,
+};
+
+/* Search strategies (the reference's strategy types and their default post-processors). */
+enum dk_strategy {
+  DK_STRATEGY_FULL_PRECISION = 0, /* FullPrecision: FP32 traversal, FilterStartPoints + copy */
+  DK_STRATEGY_HYBRID = 1,         /* Hybrid: PQ traversal, FilterStartPoints + FP32 Rerank  */
+  DK_STRATEGY_QUANTIZED = 2,      /* Quantized: PQ traversal, FilterStartPoints + copy      */
+};
+
+/* Status codes.  1..4 mirror `KnnSearchError` (diskann/src/graph/search/knn_search.rs:39-44). */
+enum dk_status {
+  DK_OK = 0,
+  DK_ERR_K_ZERO = 1,
+  DK_ERR_L_ZERO = 2,
+  DK_ERR_L_LESS_THAN_K = 3,
+  DK_ERR_BEAM_WIDTH_ZERO = 4,
+  DK_ERR_NO_PQ = 5,              /* PQ strategy on an index created without PQ data */
+  DK_ERR_INVALID_ARGUMENT = 6,   /* null pointer, zero dimension, unsupported size */
+  DK_ERR_INVALID_GRAPH = 7,      /* neighbour id out of range or degree above max_degree */
+  DK_ERR_DIMENSION_MISMATCH = 8,
+  DK_ERR_OUT_OF_MEMORY = 9,
+  DK_ERR_CUDA = 10,
+  DK_ERR_DEVICE_TIMEOUT = 11,    /* a bounded device-side wait gave up */
+  DK_ERR_UNSUPPORTED = 12,
+  DK_ERR_ADMISSION = 13,         /* serving loop: request rejected (no slot / memory) */
+  DK_ERR_CANCELLED = 14,
+  DK_ERR_NOT_FOUND = 15,
+};
+
+/* Per-query statistics: the reference's `SearchStats` (diskann/src/graph/index.rs:90-102). */
+typedef struct dk_search_stats {
+  uint32_t cmps;         /* distance computations, start points included */
+  uint32_t hops;         /* expanded nodes */
+  uint32_t result_count; /* results written (<= k) */
+  uint32_t flags;        /* internal: bit 0 = visited set spilled to the global-memory pass */
+} dk_search_stats;
+
+/* Host-side description of an in-memory index.  All arrays are host memory with
+ * num_points + num_frozen rows; dk_index_create copies them to device memory and the
+ * caller keeps ownership. */
+typedef struct dk_index_desc {
+  uint32_t num_points;        /* N data points */
+  uint32_t num_frozen;        /* F >= 1 frozen start points, ids N..N+F-1 */
+  uint32_t dim;               /* D */
+  int32_t metric;             /* enum dk_metric */
+  const float* vectors;       /* (N+F) rows of `vector_stride` floats; first D used */
+  uint64_t vector_stride;
+  const uint32_t* adjacency;  /* (N+F) rows of `adjacency_stride` ids */
+  uint64_t adjacency_stride;
+  const uint32_t* degrees;    /* (N+F) list lengths, each <= max_degree */
+  uint32_t max_degree;        /* adjacency slot width (the reference's max_degree with slack) */
+  /* Optional product quantisation (pq_chunks == 0: none).  Layout of the reference's
+   * FixedChunkPQTable (diskann-providers/src/model/pq/fixed_chunk_pq_table.rs:100-133). */
+  uint32_t pq_chunks;         /* M */
+  const uint32_t* pq_offsets; /* M+1 dimension offsets, 0 .. D, strictly increasing */
+  const float* pq_pivots;     /* 256 x D, row-major */
+  const uint8_t* pq_codes;    /* (N+F) rows of `pq_code_stride` bytes, first M used */
+  uint64_t pq_code_stride;
+} dk_index_desc;
+
+typedef struct dk_index dk_index;
+
+typedef struct dk_index_info {
+  uint32_t num_points, num_frozen, dim, max_degree, pq_chunks;
+  int32_t metric;
+  int32_t device;
+  uint64_t device_bytes;       /* HBM held by the index */
+} dk_index_info;
+
+/* Library ABI version (DK_ABI_VERSION). */
+int32_t dk_abi_version(void);
+
+/* Message of the calling thread's most recent error (NUL-terminated, truncated to len).
+ * Returns the status that produced it. */
+int32_t dk_last_error(char* buf, uint64_t len);
+
+/* `Knn::new` validation (diskann/src/graph/search/knn_search.rs:94-119). */
+int32_t dk_knn_validate(uint32_t k, uint32_t l, uint32_t beam_width);
+
+/* Build a device-resident index from host arrays (replaces constructing a
+ * `DefaultProvider` + `DiskANNIndex`, inmem/provider.rs:301-352 and index.rs:59-66). */
+int32_t dk_index_create(const dk_index_desc* desc, int32_t device, dk_index** out);
+int32_t dk_index_destroy(dk_index* index);
+int32_t dk_index_get_info(const dk_index* index, dk_index_info* info);
+
+/* Batched k-NN search with HOST buffers: copies the queries in, searches, copies results
+ * out and returns when they are in `ids`, `dists`, `stats` (stats may be NULL).
+ * Replaces `nq` calls of DiskANNIndex::search with Knn{k, l, beam_width}
+ * (diskann/src/graph/index.rs:2034-2070). */
+int32_t dk_search(dk_index* index, int32_t strategy, const float* queries, uint64_t query_stride,
+                  uint32_t nq, uint32_t k, uint32_t l, uint32_t beam_width, uint32_t* ids,
+                  float* dists, dk_search_stats* stats);
+
+/* Same search with DEVICE buffers, asynchronous on `stream` (a cudaStream_t; NULL = the
+ * legacy default stream).  `stats` is required here: the visited-set spill pass reads it. */
+int32_t dk_search_device(dk_index* index, int32_t strategy, const float* queries,
+                         uint64_t query_stride, uint32_t nq, uint32_t k, uint32_t l,
+                         uint32_t beam_width, uint32_t* ids, float* dists,
+                         dk_search_stats* stats, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DISKANN_B200_H */

@@ -1,0 +1,191 @@
+"""ctypes front-end of the CPU oracle — TEST INFRASTRUCTURE ONLY.
+
+The oracle (oracle.cpp) restates the reference's greedy beam search on the CPU.  Only the
+tests, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg use it, always as
+the checker or the timed CPU baseline, never as the product path.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+import threading
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+_lock = threading.Lock()
+_lib = None
+
+METRIC_COSINE = 0
+METRIC_INNER_PRODUCT = 1
+METRIC_L2 = 2
+METRIC_COSINE_NORMALIZED = 3
+
+STRATEGY_FULL_PRECISION = 0
+STRATEGY_HYBRID = 1
+STRATEGY_QUANTIZED = 2
+
+INVALID_ID = 0xFFFFFFFF
+
+
+class _Index(ctypes.Structure):
+    _fields_ = [
+        ("num_points", ctypes.c_uint32),
+        ("num_frozen", ctypes.c_uint32),
+        ("dim", ctypes.c_uint32),
+        ("metric", ctypes.c_int32),
+        ("vectors", ctypes.c_void_p),
+        ("vector_stride", ctypes.c_uint32),
+        ("adjacency", ctypes.c_void_p),
+        ("degrees", ctypes.c_void_p),
+        ("adjacency_stride", ctypes.c_uint32),
+        ("max_degree", ctypes.c_uint32),
+        ("pq_chunks", ctypes.c_uint32),
+        ("pq_offsets", ctypes.c_void_p),
+        ("pq_pivots", ctypes.c_void_p),
+        ("pq_codes", ctypes.c_void_p),
+        ("pq_code_stride", ctypes.c_uint32),
+    ]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("cmps", ctypes.c_uint32),
+        ("hops", ctypes.c_uint32),
+        ("result_count", ctypes.c_uint32),
+        ("flags", ctypes.c_uint32),
+    ]
+
+
+STATS_DTYPE = np.dtype(
+    [("cmps", np.uint32), ("hops", np.uint32), ("result_count", np.uint32), ("flags", np.uint32)]
+)
+
+
+def build() -> str:
+    """Compile the oracle (g++) if it is missing or stale; return the library path."""
+    src = [os.path.join(_HERE, f) for f in ("oracle.cpp", "oracle.h", "Makefile")]
+    if os.path.exists(_LIB_PATH) and all(
+        os.path.getmtime(_LIB_PATH) >= os.path.getmtime(s) for s in src
+    ):
+        return _LIB_PATH
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    with _lock:
+        if _lib is None:
+            build()
+            L = ctypes.CDLL(_LIB_PATH)
+            L.orc_distance.restype = ctypes.c_float
+            L.orc_distance.argtypes = [ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32]
+            L.orc_validate_knn.restype = ctypes.c_int32
+            L.orc_validate_knn.argtypes = [ctypes.c_uint32] * 3
+            L.orc_search.restype = ctypes.c_int32
+            L.orc_search_batch.restype = ctypes.c_int32
+            L.orc_search_batch.argtypes = [
+                ctypes.POINTER(_Index), ctypes.c_int32, ctypes.c_void_p, ctypes.c_uint32,
+                ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
+            ]
+            L.orc_bruteforce_f64.restype = None
+            L.orc_bruteforce_f64.argtypes = [
+                ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int32,
+                ctypes.c_void_p, ctypes.c_void_p,
+            ]
+            L.orc_pq_table.restype = None
+            L.orc_pq_table.argtypes = [ctypes.POINTER(_Index), ctypes.c_void_p, ctypes.c_void_p]
+            _lib = L
+    return _lib
+
+
+def _ptr(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data
+
+
+def distance(metric: int, x: np.ndarray, y: np.ndarray) -> float:
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    y = np.ascontiguousarray(y, dtype=np.float32)
+    assert x.shape == y.shape
+    return float(lib().orc_distance(metric, _ptr(x), _ptr(y), x.size))
+
+
+class OracleIndex:
+    """CPU oracle over host arrays laid out as the GPU index's inputs.
+
+    ``vectors``: (N + F, D) float32; ``adjacency``: (N + F, S) uint32 with ``degrees`` (N + F,)
+    giving each list's length; ids N..N+F-1 are the frozen start points.
+    """
+
+    def __init__(self, vectors, adjacency, degrees, num_points, metric,
+                 pq_offsets=None, pq_pivots=None, pq_codes=None):
+        self.vectors = np.ascontiguousarray(vectors, dtype=np.float32)
+        self.adjacency = np.ascontiguousarray(adjacency, dtype=np.uint32)
+        self.degrees = np.ascontiguousarray(degrees, dtype=np.uint32)
+        total = self.vectors.shape[0]
+        assert self.adjacency.shape[0] == total and self.degrees.shape[0] == total
+        self.num_points = int(num_points)
+        self.num_frozen = total - self.num_points
+        self.dim = self.vectors.shape[1]
+        self.metric = int(metric)
+        self.pq_offsets = None if pq_offsets is None else np.ascontiguousarray(pq_offsets, dtype=np.uint32)
+        self.pq_pivots = None if pq_pivots is None else np.ascontiguousarray(pq_pivots, dtype=np.float32)
+        self.pq_codes = None if pq_codes is None else np.ascontiguousarray(pq_codes, dtype=np.uint8)
+        s = _Index()
+        s.num_points = self.num_points
+        s.num_frozen = self.num_frozen
+        s.dim = self.dim
+        s.metric = self.metric
+        s.vectors = _ptr(self.vectors)
+        s.vector_stride = self.dim
+        s.adjacency = _ptr(self.adjacency)
+        s.degrees = _ptr(self.degrees)
+        s.adjacency_stride = self.adjacency.shape[1]
+        s.max_degree = self.adjacency.shape[1]
+        if self.pq_codes is not None:
+            s.pq_chunks = len(self.pq_offsets) - 1
+            s.pq_offsets = _ptr(self.pq_offsets)
+            s.pq_pivots = _ptr(self.pq_pivots)
+            s.pq_codes = _ptr(self.pq_codes)
+            s.pq_code_stride = self.pq_codes.shape[1]
+        self._s = s
+
+    def search(self, queries, k, l, beam_width=1, strategy=STRATEGY_FULL_PRECISION, threads=1):
+        q = np.ascontiguousarray(np.atleast_2d(queries), dtype=np.float32)
+        nq = q.shape[0]
+        ids = np.empty((nq, k), dtype=np.uint32)
+        dists = np.empty((nq, k), dtype=np.float32)
+        stats = np.zeros(nq, dtype=STATS_DTYPE)
+        rc = lib().orc_search_batch(
+            ctypes.byref(self._s), strategy, _ptr(q), q.shape[1], nq, k, l, beam_width,
+            _ptr(ids), _ptr(dists), _ptr(stats), threads,
+        )
+        if rc != 0:
+            raise ValueError(f"oracle search failed with status {rc}")
+        return ids, dists, stats
+
+    def pq_table(self, query):
+        q = np.ascontiguousarray(query, dtype=np.float32)
+        out = np.empty((len(self.pq_offsets) - 1, 256), dtype=np.float32)
+        lib().orc_pq_table(ctypes.byref(self._s), _ptr(q), _ptr(out))
+        return out
+
+
+def validate_knn(k: int, l: int, beam_width: int) -> int:
+    return int(lib().orc_validate_knn(k, l, beam_width))
+
+
+def bruteforce_f64(base, queries, k, metric):
+    base = np.ascontiguousarray(base, dtype=np.float32)
+    q = np.ascontiguousarray(np.atleast_2d(queries), dtype=np.float32)
+    ids = np.empty((q.shape[0], k), dtype=np.uint32)
+    d = np.empty((q.shape[0], k), dtype=np.float64)
+    lib().orc_bruteforce_f64(_ptr(base), base.shape[0], base.shape[1], base.shape[1], _ptr(q),
+                             q.shape[0], k, metric, _ptr(ids), _ptr(d))
+    return ids, d

@@ -1,0 +1,74 @@
+"""Extract the reference's grid-search and flat-kNN regression baselines into compact fixtures.
+
+The reference pins its greedy beam search with checked-in JSON baselines produced by
+``diskann/src/graph/test/cases/grid_search.rs:86-218`` (exact result ids and distances,
+comparison and hop counts for Knn(k=10, L=10, beam 1/2/4) on 1-D, 3-D and 4-D lattices) and
+its brute-force search with ``diskann/src/flat/test/cases/flat_knn_search.rs``.
+
+This script reads those files from a checkout of the reference and keeps only the fields the
+tests compare.  Run it from the repository root:
+
+    python tests/golden/make_golden.py /path/to/reference
+
+It writes ``tests/golden/grid_search.json`` and ``tests/golden/flat_knn_search.json``.
+"""
+
+import json
+import os
+import sys
+
+GRID_DIR = "diskann/test/generated/graph/test/cases/grid_search"
+FLAT_DIR = "diskann/test/generated/flat/test/cases/flat_knn_search"
+GRID_FILES = ["search_1_100.json", "search_3_5.json", "search_4_4.json"]
+FLAT_FILES = ["search_1_100.json", "search_2_5.json", "search_3_4.json"]
+
+
+def main(ref_root: str) -> None:
+    out_dir = os.path.dirname(os.path.abspath(__file__))
+
+    grid = []
+    for name in GRID_FILES:
+        with open(os.path.join(ref_root, GRID_DIR, name)) as f:
+            doc = json.load(f)
+        for case in doc["payload"]:
+            grid.append(
+                {
+                    "source": f"{GRID_DIR}/{name}",
+                    "grid_dims": case["grid_dims"],
+                    "grid_size": case["grid_size"],
+                    "beam_width": case["beam_width"],
+                    "k": 10,
+                    "l": 10,
+                    "query": case["query"],
+                    "results": case["results"],
+                    "comparisons": case["comparisons"],
+                    "hops": case["hops"],
+                    "num_results": case["num_results"],
+                }
+            )
+    with open(os.path.join(out_dir, "grid_search.json"), "w") as f:
+        json.dump(grid, f, indent=1)
+
+    flat = []
+    for name in FLAT_FILES:
+        with open(os.path.join(ref_root, FLAT_DIR, name)) as f:
+            doc = json.load(f)
+        for case in doc["payload"]:
+            flat.append(
+                {
+                    "source": f"{FLAT_DIR}/{name}",
+                    "grid_dims": case["grid_dims"],
+                    "grid_size": case["grid_size"],
+                    "k": case["k"],
+                    "query": case["query"],
+                    "ground_truth": case["ground_truth"],
+                    "result_count": case["result_count"],
+                }
+            )
+    with open(os.path.join(out_dir, "flat_knn_search.json"), "w") as f:
+        json.dump(flat, f, indent=1)
+    print(f"wrote {len(grid)} grid cases and {len(flat)} flat cases to {out_dir}")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

@@ -1,0 +1,185 @@
+"""GPU parity: the CUDA search through the C ABI against the oracle and the golden vectors.
+
+Bar: bit-exact ids, distances (float32 bit patterns), comparison and hop counts for the
+full-precision path and the PQ paths (the kernels restate the reference's float rounding
+sequence, so there is no tolerance to apply).
+"""
+
+import json
+import os
+
+import numpy as np
+import pytest
+
+from diskann_b200 import (ANNError, DiskANNIndex, FullPrecision, GpuProvider, Hybrid, Knn,
+                          Metric, PQData, Quantized, Status, datasets)
+from oracle import oracle as O
+from tests.helpers import queries_like, random_index, simple_pq
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+STRAT = {"full": (FullPrecision(), O.STRATEGY_FULL_PRECISION),
+         "hybrid": (Hybrid(), O.STRATEGY_HYBRID),
+         "quantized": (Quantized(), O.STRATEGY_QUANTIZED)}
+
+
+def _grid_cases():
+    with open(os.path.join(GOLDEN, "grid_search.json")) as f:
+        return json.load(f)
+
+
+def assert_same(gpu, orc, check_stats=True):
+    gi, gd, gs = gpu
+    oi, od, os_ = orc
+    np.testing.assert_array_equal(gi, oi)
+    np.testing.assert_array_equal(gd.view(np.uint32), od.view(np.uint32))
+    if check_stats:
+        np.testing.assert_array_equal(gs["cmps"], os_["cmps"])
+        np.testing.assert_array_equal(gs["hops"], os_["hops"])
+        np.testing.assert_array_equal(gs["result_count"], os_["result_count"])
+
+
+@pytest.mark.parametrize("case", _grid_cases(),
+                         ids=lambda c: f"d{c['grid_dims']}s{c['grid_size']}b{c['beam_width']}q{c['query'][0]:g}")
+def test_grid_golden_through_abi(case):
+    v, a, d, n = datasets.grid(case["grid_dims"], case["grid_size"])
+    idx = DiskANNIndex(GpuProvider(v, a, d, n, Metric.L2))
+    ids, dists, st = idx.search(Knn(case["k"], case["l"], case["beam_width"]), FullPrecision(),
+                                np.array([case["query"]], np.float32))
+    assert [int(i) for i in ids[0]] == [r[0] for r in case["results"]]
+    assert [float(x) for x in dists[0]] == [r[1] for r in case["results"]]
+    assert int(st[0]["cmps"]) == case["comparisons"]
+    assert int(st[0]["hops"]) == case["hops"]
+    assert int(st[0]["result_count"]) == case["num_results"]
+
+
+@pytest.mark.parametrize("metric", [Metric.L2, Metric.INNER_PRODUCT, Metric.COSINE,
+                                    Metric.COSINE_NORMALIZED])
+@pytest.mark.parametrize("dim", [3, 100, 128])
+@pytest.mark.parametrize("beam", [1, 4])
+def test_full_precision_parity(metric, dim, beam):
+    norm = metric in (Metric.COSINE_NORMALIZED, Metric.INNER_PRODUCT)
+    v, a, d, n = random_index(3000, dim, 24, seed=dim + beam, normalize=norm, max_degree=31)
+    q = queries_like(v[:n], 64, seed=11, normalize=norm)
+    idx = DiskANNIndex(GpuProvider(v, a, d, n, metric))
+    orc = O.OracleIndex(v, a, d, n, int(metric))
+    for k, l in [(10, 10), (10, 64), (1, 128)]:
+        gpu = idx.search(Knn(k, l, beam), FullPrecision(), q)
+        assert_same(gpu, orc.search(q, k, l, beam, O.STRATEGY_FULL_PRECISION, threads=4))
+
+
+@pytest.mark.parametrize("dim", [96, 384, 768])
+def test_full_precision_parity_benchmark_dims(dim):
+    v, a, d, n = random_index(2000, dim, 20, seed=dim, max_degree=26)
+    q = queries_like(v[:n], 32, seed=5)
+    idx = DiskANNIndex(GpuProvider(v, a, d, n, Metric.L2))
+    orc = O.OracleIndex(v, a, d, n, O.METRIC_L2)
+    gpu = idx.search(Knn(10, 100), FullPrecision(), q)
+    assert_same(gpu, orc.search(q, 10, 100, 1, O.STRATEGY_FULL_PRECISION, threads=4))
+
+
+@pytest.mark.parametrize("metric", [Metric.L2, Metric.INNER_PRODUCT, Metric.COSINE_NORMALIZED])
+@pytest.mark.parametrize("strategy", ["hybrid", "quantized"])
+def test_pq_parity(metric, strategy):
+    norm = metric != Metric.L2
+    v, a, d, n = random_index(3000, 64, 24, seed=21, normalize=norm, max_degree=31)
+    off, piv, codes = simple_pq(v, 16, seed=22)
+    q = queries_like(v[:n], 48, seed=23, normalize=norm)
+    idx = DiskANNIndex(GpuProvider(v, a, d, n, metric, pq=PQData(off, piv, codes)))
+    orc = O.OracleIndex(v, a, d, n, int(metric), off, piv, codes)
+    s, os_ = STRAT[strategy]
+    for k, l, bw in [(10, 50, 1), (10, 100, 2), (5, 200, 1)]:
+        assert_same(idx.search(Knn(k, l, bw), s, q), orc.search(q, k, l, bw, os_, threads=4))
+
+
+def test_spill_pass_is_exact(monkeypatch):
+    """A visited set forced past its shared-memory hash runs in the bitmap pass, same results."""
+    v, a, d, n = random_index(4000, 32, 30, seed=31, max_degree=30)
+    q = queries_like(v[:n], 40, seed=32)
+    idx = DiskANNIndex(GpuProvider(v, a, d, n, Metric.L2))
+    orc = O.OracleIndex(v, a, d, n, O.METRIC_L2)
+    ref = orc.search(q, 10, 200, 1, O.STRATEGY_FULL_PRECISION, threads=4)
+    monkeypatch.setenv("DK_HASH_LOG2", "8")
+    gpu = idx.search(Knn(10, 200), FullPrecision(), q)
+    assert (gpu[2]["flags"] & 1).any()
+    assert_same(gpu, ref)
+    monkeypatch.delenv("DK_HASH_LOG2")
+    gpu2 = idx.search(Knn(10, 200), FullPrecision(), q)
+    assert_same(gpu2, ref)
+
+
+def test_multiple_frozen_points_and_duplicates():
+    """Two start points; adjacency lists with repeated ids (the visited set drops repeats)."""
+    v, a, d, n = random_index(1500, 16, 12, seed=41, frozen=2, max_degree=16)
+    rng = np.random.default_rng(42)
+    for r in rng.choice(n, 200, replace=False):
+        if d[r] < 16:
+            a[r, d[r]] = a[r, 0]
+            d[r] += 1
+    q = queries_like(v[:n], 32, seed=43)
+    idx = DiskANNIndex(GpuProvider(v, a, d, n, Metric.L2))
+    orc = O.OracleIndex(v, a, d, n, O.METRIC_L2)
+    assert_same(idx.search(Knn(10, 40, 2), FullPrecision(), q),
+                orc.search(q, 10, 40, 2, O.STRATEGY_FULL_PRECISION))
+
+
+def test_nan_vectors_are_scored_not_inserted():
+    v, a, d, n = random_index(800, 8, 10, seed=51, max_degree=10)
+    v[::7, 3] = np.nan
+    q = queries_like(np.nan_to_num(v[:n]), 16, seed=52)
+    idx = DiskANNIndex(GpuProvider(v, a, d, n, Metric.L2))
+    orc = O.OracleIndex(v, a, d, n, O.METRIC_L2)
+    assert_same(idx.search(Knn(10, 30), FullPrecision(), q),
+                orc.search(q, 10, 30, 1, O.STRATEGY_FULL_PRECISION))
+
+
+def test_k_equals_l_and_small_graph():
+    v, a, d, n = random_index(50, 4, 6, seed=61, max_degree=6)
+    q = queries_like(v[:n], 8, seed=62)
+    idx = DiskANNIndex(GpuProvider(v, a, d, n, Metric.L2))
+    orc = O.OracleIndex(v, a, d, n, O.METRIC_L2)
+    for k, l in [(1, 1), (7, 7), (50, 60)]:
+        assert_same(idx.search(Knn(k, l), FullPrecision(), q),
+                    orc.search(q, k, l, 1, O.STRATEGY_FULL_PRECISION))
+
+
+def test_device_entry_point_matches_host_entry_point():
+    import torch
+
+    v, a, d, n = random_index(2000, 64, 16, seed=71, max_degree=20)
+    q = queries_like(v[:n], 100, seed=72)
+    idx = DiskANNIndex(GpuProvider(v, a, d, n, Metric.L2))
+    hi, hd, hs = idx.search(Knn(10, 50), FullPrecision(), q)
+    dq = torch.from_numpy(q).cuda()
+    ids = torch.empty((100, 10), dtype=torch.int32, device="cuda")
+    dists = torch.empty((100, 10), dtype=torch.float32, device="cuda")
+    st = torch.empty((100, 4), dtype=torch.int32, device="cuda")
+    idx.search_device(Knn(10, 50), FullPrecision(), dq, ids, dists, st)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(ids.cpu().numpy().view(np.uint32), hi)
+    np.testing.assert_array_equal(dists.cpu().numpy(), hd)
+    np.testing.assert_array_equal(st.cpu().numpy()[:, 0].view(np.uint32), hs["cmps"])
+
+
+def test_errors():
+    v, a, d, n = random_index(100, 8, 6, seed=81, max_degree=6)
+    bad = a.copy()
+    bad[3, 0] = 10_000
+    with pytest.raises(ANNError) as ei:
+        GpuProvider(v, bad, d, n, Metric.L2)
+    assert ei.value.status == Status.INVALID_GRAPH
+    d2 = d.copy()
+    d2[5] = 7
+    with pytest.raises(ANNError) as ei:
+        GpuProvider(v, a, d2, n, Metric.L2)
+    assert ei.value.status == Status.INVALID_GRAPH
+    idx = DiskANNIndex(GpuProvider(v, a, d, n, Metric.L2))
+    with pytest.raises(ANNError) as ei:
+        idx.search(Knn(5, 10), Hybrid(), v[:2])
+    assert ei.value.status == Status.NO_PQ
+    with pytest.raises(ANNError) as ei:
+        idx.search(Knn(5, 10), FullPrecision(), v[:2, :4])
+    assert ei.value.status == Status.DIMENSION_MISMATCH
+    ids, dists, st = idx.search(Knn(5, 10), FullPrecision(), np.zeros((0, 8), np.float32))
+    assert ids.shape == (0, 5)

@@ -1,0 +1,111 @@
+"""CPU: pin the oracle against the reference's golden vectors and basic invariants."""
+
+import json
+import os
+
+import numpy as np
+import pytest
+
+from diskann_b200 import datasets
+from oracle import oracle as O
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _grid_cases():
+    with open(os.path.join(GOLDEN, "grid_search.json")) as f:
+        return json.load(f)
+
+
+@pytest.mark.parametrize("case", _grid_cases(),
+                         ids=lambda c: f"d{c['grid_dims']}s{c['grid_size']}b{c['beam_width']}q{c['query'][0]:g}")
+def test_oracle_matches_grid_golden(case):
+    """Exact ids, distances, comparisons and hops of grid_search.rs's baselines."""
+    v, a, d, n = datasets.grid(case["grid_dims"], case["grid_size"])
+    ix = O.OracleIndex(v, a, d, n, O.METRIC_L2)
+    ids, dists, st = ix.search(np.array(case["query"], np.float32), case["k"], case["l"],
+                               case["beam_width"])
+    assert [int(i) for i in ids[0]] == [r[0] for r in case["results"]]
+    assert [float(x) for x in dists[0]] == [r[1] for r in case["results"]]
+    assert int(st[0]["cmps"]) == case["comparisons"]
+    assert int(st[0]["hops"]) == case["hops"]
+    assert int(st[0]["result_count"]) == case["num_results"]
+
+
+def test_flat_golden_bruteforce():
+    """The f64 brute force reproduces flat_knn_search's ground truth (as distance lists;
+    ties may be listed in another order)."""
+    with open(os.path.join(GOLDEN, "flat_knn_search.json")) as f:
+        cases = json.load(f)
+    for c in cases:
+        v, _, _, n = datasets.grid(c["grid_dims"], c["grid_size"])
+        ids, d = O.bruteforce_f64(v[:n], np.array(c["query"], np.float32), c["k"], O.METRIC_L2)
+        cnt = c["result_count"]
+        gt = c["ground_truth"]
+        assert [float(x) for x in d[0][:cnt]] == [g[1] for g in gt]
+        # Same id sets within each distance value.
+        for dist in set(g[1] for g in gt):
+            exp = {g[0] for g in gt if g[1] == dist}
+            got = {int(i) for i, x in zip(ids[0][:cnt], d[0][:cnt]) if x == dist}
+            if dist != max(g[1] for g in gt):
+                assert exp == got
+
+
+@pytest.mark.parametrize("k,l,bw,status", [(0, 10, 1, 1), (1, 0, 1, 2), (11, 10, 1, 3),
+                                           (10, 10, 0, 4), (10, 10, 1, 0)])
+def test_oracle_knn_validation(k, l, bw, status):
+    assert O.validate_knn(k, l, bw) == status
+
+
+@pytest.mark.parametrize("dim", [1, 3, 7, 8, 13, 32, 40, 96, 100, 128, 384, 768])
+def test_oracle_distances_close_to_f64(dim):
+    rng = np.random.default_rng(dim)
+    x = rng.standard_normal(dim).astype(np.float32)
+    y = rng.standard_normal(dim).astype(np.float32)
+    x64, y64 = x.astype(np.float64), y.astype(np.float64)
+    l2 = ((x64 - y64) ** 2).sum()
+    ip = (x64 * y64).sum()
+    cos = ip / np.sqrt((x64 * x64).sum() * (y64 * y64).sum())
+    assert O.distance(O.METRIC_L2, x, y) == pytest.approx(l2, rel=1e-5)
+    assert O.distance(O.METRIC_INNER_PRODUCT, x, y) == pytest.approx(-ip, rel=1e-4, abs=1e-4)
+    assert O.distance(O.METRIC_COSINE, x, y) == pytest.approx(1 - cos, rel=1e-4, abs=1e-5)
+    assert O.distance(O.METRIC_COSINE_NORMALIZED, x, y) == pytest.approx(1 - ip, rel=1e-4, abs=1e-4)
+
+
+def test_oracle_cosine_zero_norm():
+    """A norm below f32::MIN_POSITIVE gives similarity 0 (simd.rs:2355-2357)."""
+    x = np.zeros(16, np.float32)
+    y = np.ones(16, np.float32)
+    assert O.distance(O.METRIC_COSINE, x, y) == 1.0
+
+
+def test_oracle_pq_table_matches_direct():
+    """ADC lookup equals the sum of per-chunk direct distances (pq/distance/dynamic.rs tests)."""
+    from tests.helpers import random_index, simple_pq
+
+    v, a, d, n = random_index(300, 32, 8, seed=3)
+    off, piv, codes = simple_pq(v, 8, seed=4)
+    ix = O.OracleIndex(v, a, d, n, O.METRIC_L2, off, piv, codes)
+    q = v[5] + 0.5
+    table = ix.pq_table(q)
+    for m in range(8):
+        s, e = off[m], off[m + 1]
+        for c in (0, 17, 255):
+            ref = float(((q[s:e].astype(np.float64) - piv[c, s:e]) ** 2).sum())
+            assert table[m, c] == pytest.approx(ref, rel=1e-5, abs=1e-6)
+
+
+def test_oracle_search_finds_exact_on_complete_graph():
+    """With a complete graph and L >= N every point is scored, so results are exact."""
+    rng = np.random.default_rng(0)
+    n, dim = 40, 8
+    base = rng.standard_normal((n, dim)).astype(np.float32)
+    vectors = np.vstack([base, base[:1]])
+    adj = np.array([[j for j in range(n + 1) if j != i][: n] for i in range(n + 1)], np.uint32)
+    deg = np.full(n + 1, n, np.uint32)
+    ix = O.OracleIndex(vectors, adj, deg, n, O.METRIC_L2)
+    q = rng.standard_normal(dim).astype(np.float32)
+    ids, dists, st = ix.search(q, 5, 50)
+    gt, _ = O.bruteforce_f64(base, q, 5, O.METRIC_L2)
+    assert list(ids[0]) == list(gt[0])
+    assert st[0]["cmps"] == n + 1
