@@ -23,6 +23,11 @@ EXPORTED_SYMBOLS = (
     "dk_index_get_info",
     "dk_search",
     "dk_search_device",
+    "dk_distance",
+    "dk_compute_medoid",
+    "dk_build_vamana",
+    "dk_pq_train",
+    "dk_pq_encode",
 )
 
 

@@ -26,7 +26,8 @@ NVCC_FLAGS = ARCH + [
     "-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC",
     "-Xcompiler", "-O2", "-I", os.path.join(_ROOT, "include"), "-I", CSRC,
 ]
-CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-pthread", "-I", os.path.join(_ROOT, "include"),
+# x86-64-v3 (AVX2 + FMA) like the reference's own target; no contraction beyond explicit fma.
+CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-pthread", "-mavx2", "-mfma", "-ffp-contract=off", "-I", os.path.join(_ROOT, "include"),
              "-I", CSRC, "-I", "/usr/local/cuda/include"]
 
 

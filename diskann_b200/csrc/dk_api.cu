@@ -41,6 +41,7 @@ void free_index(dk_index* ix) {
   cudaFree(ix->codes);
   cudaFree(ix->pivots);
   cudaFree(ix->offsets);
+  if (ix->hint_host) cudaFreeHost(ix->hint_host);
   cudaSetDevice(prev);
   delete ix;
 }
@@ -203,6 +204,13 @@ extern "C" int32_t dk_index_create(const dk_index_desc* d, int32_t device, dk_in
       e = upload(reinterpret_cast<void**>(&ix->pivots), d->pq_pivots, (size_t)256 * d->dim * sizeof(float));
     if (e == cudaSuccess)
       e = upload(reinterpret_cast<void**>(&ix->offsets), d->pq_offsets, (d->pq_chunks + 1) * sizeof(uint32_t));
+  }
+  if (e == cudaSuccess) {
+    e = cudaHostAlloc(reinterpret_cast<void**>(&ix->hint_host), 2 * sizeof(uint32_t), cudaHostAllocMapped);
+    if (e == cudaSuccess) {
+      ix->hint_host[0] = ix->hint_host[1] = 0u;
+      e = cudaHostGetDevicePointer(reinterpret_cast<void**>(&ix->hint_dev), ix->hint_host, 0);
+    }
   }
   if (e != cudaSuccess) {
     free_index(ix);

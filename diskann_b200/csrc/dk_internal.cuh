@@ -26,6 +26,11 @@ struct dk_index {
   float* pivots = nullptr;
   uint32_t* offsets = nullptr;
   uint64_t bytes = 0;
+  // Visited-set sizing hint in mapped pinned host memory: word 0 = largest
+  // cmps * 256 / (L + F) seen by kernels since the last launch read it, word 1 = the value the
+  // last launch used.  Only performance depends on it (an undersized hash spills, exactly).
+  uint32_t* hint_host = nullptr;
+  uint32_t* hint_dev = nullptr;
 };
 
 // Per-launch parameters of the beam-search kernels.
@@ -54,6 +59,7 @@ struct SearchParams {
   uint32_t off_cand_id, off_cand_d, off_new_d, off_new_id, off_hash, off_misc;
   uint32_t smem_bytes;
   uint32_t list_cap;  // capacity of the candidate / rerank lists
+  uint32_t* hint;     // device view of dk_index::hint_host (may be null)
 };
 
 constexpr uint32_t kFlagSpilled = 1u;

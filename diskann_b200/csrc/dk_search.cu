@@ -634,6 +634,7 @@ __global__ void __launch_bounds__(NT) k_search_hash(const SearchParams P) {
   if (threadIdx.x == 0) {
     dk_search_stats st = {cmps, hops, S.misc->pad, 0u};
     P.stats[qid] = st;
+    if (P.hint) atomicMax(P.hint, (uint32_t)(((uint64_t)cmps << 8) / P.cap));
   }
 }
 
@@ -655,6 +656,7 @@ __global__ void __launch_bounds__(NT) k_search_spill(const SearchParams P) {
     if (threadIdx.x == 0) {
       dk_search_stats st = {cmps, hops, S.misc->pad, kFlagSpilled};
       P.stats[qid] = st;
+      if (P.hint) atomicMax(P.hint, (uint32_t)(((uint64_t)cmps << 8) / P.cap));
     }
     __syncthreads();
   }
@@ -777,12 +779,26 @@ int32_t dk_launch_search(const dk_index* ix, int32_t strategy, const float* quer
   P.stats = stats;
   P.list_cap = std::max(std::max(beam * ix->max_degree, P.cap), ix->f);
 
-  // Visited-set hash: sized from the reference's own visited-set estimate
-  // (scratch.rs:186-193: 1.1 * max_degree * 1.3 * L is an upper bound for max_degree =
-  // slot width), at most half full; queries that need more spill to the bitmap pass.
-  const double est = 0.55 * ix->max_degree * (double)l + ix->f + beam * ix->max_degree;
-  uint32_t log2h = 10;
-  while ((double)(1u << log2h) * 0.5 < est && log2h < 16) ++log2h;
+  // Visited-set hash.  |visited| equals the comparison count, which for a given graph grows
+  // about linearly with L + F.  The ratio is learned from previous launches on this index
+  // (kernels record their largest cmps / (L + F) in mapped host memory); before any launch
+  // the prior is half the reference's own upper-bound estimate (scratch.rs:186-193,
+  // 1.1 * max_degree * 1.3 * L).  The hash is sized to stay under 3/4 load for the learned
+  // ratio plus one hop; a query that needs more re-runs exactly in the bitmap spill pass.
+  double ratio = 0.5 * 1.1 * 1.3 * ix->max_degree;
+  P.hint = ix->hint_dev;
+  if (ix->hint_host) {
+    volatile uint32_t* h = ix->hint_host;
+    const uint32_t seen = h[0];
+    if (seen) {
+      h[1] = seen;
+      h[0] = 0;
+    }
+    if (h[1]) ratio = (double)h[1] / 256.0 * 1.15;
+  }
+  const double est = ratio * (double)P.cap + beam * ix->max_degree + ix->f;
+  uint32_t log2h = 9;
+  while ((double)(1u << log2h) * 0.75 < est && log2h < 16) ++log2h;
   log2h = env_u32("DK_HASH_LOG2", log2h);
   if (log2h < 6) log2h = 6;
   if (log2h > 20) log2h = 20;

@@ -147,6 +147,52 @@ int32_t dk_search_device(dk_index* index, int32_t strategy, const float* queries
                          uint32_t beam_width, uint32_t* ids, float* dists,
                          dk_search_stats* stats, void* stream);
 
+
+/* ---- Data tooling on either side of the search path (host code, no GPU needed) ---- */
+
+/* Distance with the reference's float rounding sequence (x86-64-v3 kernels,
+ * diskann-vector/src/distance/simd.rs:321-363, 686-846; post-ops implementations.rs:215-405). */
+int32_t dk_distance(int32_t metric, const float* x, const float* y, uint32_t len, float* out);
+
+/* Medoid start point: index of the first row nearest (squared L2) to the f64 mean
+ * (diskann-utils/src/sampling/medoid.rs:15-45). */
+int32_t dk_compute_medoid(const float* vectors, uint64_t stride, uint32_t n, uint32_t dim,
+                          uint32_t* medoid);
+
+/* Vamana construction parameters (diskann/src/graph/config/mod.rs:182-331; defaults in
+ * config/defaults.rs: alpha 1.2, max_occlusion 750). */
+typedef struct dk_build_params {
+  uint32_t pruned_degree;  /* R */
+  uint32_t max_degree;     /* slot width, floor(1.3 R) in the reference benchmark */
+  uint32_t l_build;
+  float alpha;
+  uint32_t max_backedges;  /* ceil(backedge_ratio * R) */
+  uint32_t max_occlusion;  /* 0 = 750 */
+  uint32_t num_threads;    /* 0 = all hardware threads */
+  uint32_t max_batch;      /* 0 = max(64, N / 64) */
+} dk_build_params;
+
+/* Build a Vamana graph over `vectors` ((num_points + num_frozen) rows; the frozen rows are
+ * the start points) by deterministic batched insertion (insert / occlude_list /
+ * add_edge_and_prune, diskann/src/graph/index.rs:226-341, 2269-2346, 2570-2782).  Writes
+ * (N+F) rows of `adjacency_stride` ids and their lengths. */
+int32_t dk_build_vamana(const float* vectors, uint64_t stride, uint32_t num_points,
+                        uint32_t num_frozen, uint32_t dim, int32_t metric,
+                        const dk_build_params* params, uint32_t* adjacency,
+                        uint64_t adjacency_stride, uint32_t* degrees);
+
+/* Product-quantisation schema: 256 centres per chunk by k-means++ and Lloyd iterations on
+ * the given rows; chunk offsets split dim with the first dim % chunks chunks one longer
+ * (the reference's FixedChunkPQTable layout, fixed_chunk_pq_table.rs:100-133). */
+int32_t dk_pq_train(const float* data, uint64_t stride, uint32_t n, uint32_t dim, uint32_t chunks,
+                    uint32_t iters, uint64_t seed, uint32_t num_threads, uint32_t* offsets,
+                    float* pivots);
+
+/* Encode rows to PQ codes (nearest centre per chunk). */
+int32_t dk_pq_encode(const float* data, uint64_t stride, uint32_t n, uint32_t dim, uint32_t chunks,
+                     const uint32_t* offsets, const float* pivots, uint32_t num_threads,
+                     uint8_t* codes, uint64_t code_stride);
+
 #ifdef __cplusplus
 }
 #endif

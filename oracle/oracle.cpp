@@ -14,7 +14,7 @@
 // Every function cites the reference file:line it restates.  Paths are relative to the
 // reference repository root.
 //
-// Build: see oracle/Makefile (g++ -O2 -ffp-contract=off; no fast-math, so every float
+// Build: see oracle/Makefile (g++ -O3 -mavx2 -mfma -ffp-contract=off; no fast-math, so every float
 // operation rounds exactly as written and every fused multiply-add is an explicit fmaf).
 
 #include <algorithm>
@@ -222,6 +222,44 @@ struct Queue {
   size_t iter_len() const { return std::min(search_l, size); }
 };
 
+// Visited set: an open-addressing u32 set with linear probing that doubles at 50% load.
+// Membership semantics are those of the reference's hashbrown::HashSet<u32> (scratch.rs:41-48).
+struct VisitedSet {
+  std::vector<uint32_t> slots;
+  size_t mask = 0, count = 0;
+  explicit VisitedSet(size_t hint) {
+    size_t cap = 16;
+    while (cap < 2 * hint) cap <<= 1;
+    slots.assign(cap, 0xFFFFFFFFu);
+    mask = cap - 1;
+  }
+  static size_t hash(uint32_t id) { return (size_t)(id * 2654435761u); }
+  // Returns true if `id` was newly inserted.
+  bool insert(uint32_t id) {
+    if (2 * (count + 1) > slots.size()) grow();
+    size_t h = hash(id) & mask;
+    while (true) {
+      const uint32_t cur = slots[h];
+      if (cur == id) return false;
+      if (cur == 0xFFFFFFFFu) {
+        slots[h] = id;
+        ++count;
+        return true;
+      }
+      h = (h + 1) & mask;
+    }
+  }
+  void grow() {
+    std::vector<uint32_t> old;
+    old.swap(slots);
+    slots.assign(old.size() * 2, 0xFFFFFFFFu);
+    mask = slots.size() - 1;
+    count = 0;
+    for (uint32_t v : old)
+      if (v != 0xFFFFFFFFu) insert(v);
+  }
+};
+
 inline const float* vec_row(const orc_index* ix, uint32_t id) {
   return ix->vectors + (size_t)id * ix->vector_stride;
 }
@@ -305,8 +343,7 @@ extern "C" int32_t orc_search(const orc_index* ix, int32_t strategy, const float
 
   const uint32_t n_start = ix->num_frozen;
   Queue best((size_t)l + n_start);
-  std::unordered_set<uint32_t> visited;
-  visited.reserve((size_t)std::ceil(1.1 * ix->max_degree * 1.3 * l));
+  VisitedSet visited((size_t)std::ceil(1.1 * ix->max_degree * 1.3 * l));
   uint32_t cmps = 0, hops = 0;
 
   // search_internal: start points (index.rs:1956-1963).
@@ -333,7 +370,7 @@ extern "C" int32_t orc_search(const orc_index* ix, int32_t strategy, const float
       const uint32_t* adj = ix->adjacency + (size_t)n * ix->adjacency_stride;
       for (uint32_t t = 0; t < deg; ++t) {
         const uint32_t id = adj[t];
-        if (visited.insert(id).second) neighbors.emplace_back(id, score(id));
+        if (visited.insert(id)) neighbors.emplace_back(id, score(id));
       }
     }
     for (const auto& nb : neighbors) best.insert(nb.first, nb.second);
