@@ -40,6 +40,7 @@ void free_index(dk_index* ix) {
   cudaFree(ix->adj);
   cudaFree(ix->codes);
   cudaFree(ix->pivots);
+  cudaFree(ix->pivots_cm);
   cudaFree(ix->offsets);
   if (ix->hint_host) cudaFreeHost(ix->hint_host);
   cudaSetDevice(prev);
@@ -202,6 +203,17 @@ extern "C" int32_t dk_index_create(const dk_index_desc* d, int32_t device, dk_in
     e = upload(reinterpret_cast<void**>(&ix->codes), codes.data(), codes.size());
     if (e == cudaSuccess)
       e = upload(reinterpret_cast<void**>(&ix->pivots), d->pq_pivots, (size_t)256 * d->dim * sizeof(float));
+    if (e == cudaSuccess) {
+      // Chunk-major pivots: chunk m's 256 centres are contiguous runs of len_m floats.
+      std::vector<float> cm((size_t)256 * d->dim);
+      for (uint32_t m = 0; m < d->pq_chunks; ++m) {
+        const uint32_t s = d->pq_offsets[m], len = d->pq_offsets[m + 1] - s;
+        for (uint32_t c = 0; c < 256; ++c)
+          std::memcpy(&cm[(size_t)s * 256 + (size_t)c * len], d->pq_pivots + (size_t)c * d->dim + s,
+                      len * sizeof(float));
+      }
+      e = upload(reinterpret_cast<void**>(&ix->pivots_cm), cm.data(), cm.size() * sizeof(float));
+    }
     if (e == cudaSuccess)
       e = upload(reinterpret_cast<void**>(&ix->offsets), d->pq_offsets, (d->pq_chunks + 1) * sizeof(uint32_t));
   }

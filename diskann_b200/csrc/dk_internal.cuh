@@ -24,6 +24,7 @@ struct dk_index {
   uint32_t* adj = nullptr;
   uint8_t* codes = nullptr;
   float* pivots = nullptr;
+  float* pivots_cm = nullptr;  // chunk-major copy: chunk m, centre c -> len_m floats
   uint32_t* offsets = nullptr;
   uint64_t bytes = 0;
   // Visited-set sizing hint in mapped pinned host memory: word 0 = largest
@@ -39,6 +40,7 @@ struct SearchParams {
   const uint32_t* adj;
   const uint8_t* codes;
   const float* pivots;
+  const float* pivots_cm;
   const uint32_t* offsets;
   uint32_t n, f, dim, vstride, astride, max_degree, cstride, pq_chunks;
   const float* queries;
@@ -54,10 +56,12 @@ struct SearchParams {
   uint32_t hash_limit;  // inserts allowed before the hash counts as full
   uint32_t* bitmap;
   uint32_t bitmap_words;
-  // Shared-memory carve-up (byte offsets into dynamic shared memory).
+  // Shared-memory carve-up: byte offsets from the CTA's dynamic shared memory (CTA kernel)
+  // or from the warp's slice of it (warp kernel, slices of `warp_smem` bytes).
   uint32_t off_query, off_table, off_qd0, off_qi0, off_qd1, off_qi1;
   uint32_t off_cand_id, off_cand_d, off_new_d, off_new_id, off_hash, off_misc;
   uint32_t smem_bytes;
+  uint32_t warp_smem;
   uint32_t list_cap;  // capacity of the candidate / rerank lists
   uint32_t* hint;     // device view of dk_index::hint_host (may be null)
 };

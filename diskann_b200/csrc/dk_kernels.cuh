@@ -1,0 +1,989 @@
+// Device code of the batched greedy beam search (sm_100a).
+//
+// Two kernels run the reference's `search_internal` loop (diskann/src/graph/index.rs:
+// 1938-2005) for a batch of queries, each query's state resident in shared memory:
+//
+//  * k_search_warp — one WARP per query, several queries per CTA, no block barriers.  A
+//    hop's work is small (one adjacency row, a few to a few dozen candidates), so the kernel
+//    is bound by dependent memory latency; one warp per query keeps many queries in flight
+//    per SM and every phase is warp-synchronous (ballots, shuffles, __syncwarp).
+//  * k_search_cta — one CTA (128 threads) per query: more lanes per hop for wide rows
+//    (D >= 384) or wide beams.  Its bitmap variant is the spill pass (below).
+//
+// Query state:
+//   * the candidate queue (diskann/src/neighbor/queue.rs:68-519): sorted (distance, id) arrays
+//     with capacity L + #start points, visited flag in the id's top bit, double-buffered so a
+//     hop's candidates merge in one parallel pass;
+//   * the visited set (diskann/src/graph/search/scratch.rs:41-48, glue.rs:524-561): an
+//     open-addressing u32 hash in shared memory; a query that would load it past 3/4 is
+//     abandoned and re-run by the spill pass with an exact bitmap over all ids in global
+//     memory, so results never depend on the hash size;
+//   * the query vector and, for PQ traversal, the per-query ADC table
+//     (diskann-providers/src/model/pq/fixed_chunk_pq_table.rs:149-215).
+//
+// Full-precision scoring uses 8-lane subgroups: lane s reads float4 pieces at offsets
+// 32*b + 4*s of the row, which makes it own exactly accumulator lanes 4s..4s+3 of the
+// reference's x86-64-v3 kernel (four f32x8 accumulators over 32-float blocks,
+// diskann-vector/src/distance/simd.rs:321-363, 686-745).  The reduction then reproduces
+// the reference's rounding sequence bit for bit: (s0+s1)+(s2+s3) lane-wise, masked
+// remainder, sum_tree (diskann-wide/src/arch/x86_64/v3/f32x8_.rs:187-212).
+//
+// Merge: the reference inserts a hop's candidates one by one in adjacency order; `insert`
+// (queue.rs:130-171) places an item before existing equal distances, drops it when the queue
+// is full and its distance exceeds the last, and evicts the last otherwise.  That is the
+// first `cap` entries of the union ordered by (distance, newest first), which the merge
+// computes directly: new items are ranked among themselves by (distance ascending, adjacency
+// position descending) and placed before old items of equal distance.  NaN distances are
+// scored and counted but never inserted (queue.rs:131-135).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+
+#include "dk_internal.cuh"
+
+namespace dk {
+
+constexpr uint32_t kEmpty = 0xFFFFFFFFu;
+constexpr uint32_t kVisited = 0x80000000u;
+constexpr uint32_t kIdMask = 0x7FFFFFFFu;
+constexpr uint32_t kFull = 0xFFFFFFFFu;
+constexpr int kCtaThreads = 128;
+
+// ----------------------------------------------------------------------------------------
+// Visited sets.
+// ----------------------------------------------------------------------------------------
+
+struct SmemHashSet {
+  uint32_t* slots;
+  uint32_t mask;
+  uint32_t shift;
+
+  __device__ void clear(uint32_t tid, uint32_t nt) const {
+    for (uint32_t i = tid; i <= mask; i += nt) slots[i] = kEmpty;
+  }
+  // True if `id` was absent (and is now present).  Callers keep the load at most 3/4, so
+  // the probe always ends.
+  __device__ bool insert(uint32_t id) const {
+    volatile uint32_t* s = slots;
+    uint32_t h = (id * 2654435761u) >> shift;
+    while (true) {
+      const uint32_t cur = s[h];
+      if (cur == id) return false;
+      if (cur == kEmpty) {
+        const uint32_t old = atomicCAS(&slots[h], kEmpty, id);
+        if (old == kEmpty) return true;
+        if (old == id) return false;
+      }
+      h = (h + 1) & mask;
+    }
+  }
+};
+
+struct BitmapSet {
+  uint32_t* words;
+  uint32_t nwords;
+
+  __device__ void clear(uint32_t tid, uint32_t nt) const {
+    for (uint32_t i = tid; i < nwords; i += nt) words[i] = 0u;
+  }
+  __device__ bool insert(uint32_t id) const {
+    const uint32_t bit = 1u << (id & 31u);
+    const uint32_t old = atomicOr(&words[id >> 5], bit);
+    return (old & bit) == 0u;
+  }
+};
+
+// ----------------------------------------------------------------------------------------
+// Small helpers.
+// ----------------------------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// Exclusive prefix of a 0/1 flag over the block, in thread order; `total` = block sum.
+template <int NT>
+__device__ __forceinline__ uint32_t block_scan(bool flag, uint32_t* warp_sums, uint32_t& total) {
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t b = __ballot_sync(kFull, flag);
+  const uint32_t pre = __popc(b & lanemask_lt());
+  if (lane == 0) warp_sums[warp] = __popc(b);
+  __syncthreads();
+  uint32_t base = 0, tot = 0;
+#pragma unroll
+  for (int w = 0; w < NT / 32; ++w) {
+    const uint32_t s = warp_sums[w];
+    base += (w < (int)warp) ? s : 0u;
+    tot += s;
+  }
+  __syncthreads();
+  total = tot;
+  return base + pre;
+}
+
+// Entries of sorted a[0..n) that are < d / <= d.
+__device__ __forceinline__ uint32_t count_less(const float* a, uint32_t n, float d) {
+  uint32_t lo = 0, hi = n;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (a[mid] < d) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+__device__ __forceinline__ uint32_t count_less_equal(const float* a, uint32_t n, float d) {
+  uint32_t lo = 0, hi = n;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (a[mid] <= d) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+// ----------------------------------------------------------------------------------------
+// Distances.
+// ----------------------------------------------------------------------------------------
+
+__device__ __forceinline__ float tree4(float u0, float u1, float u2, float u3) {
+  // Each lane holds q_i = t_i + t_{i+4} (i = 0..3); sum_tree: (q0+q2) + (q1+q3).
+  const float d0 = u0 + u2, d1 = u1 + u3;
+  return d0 + d1;
+}
+
+template <int METRIC>
+__device__ __forceinline__ void acc4(float4 a, float4 v, float* acc) {
+  if (METRIC == DK_METRIC_L2) {
+    const float c0 = a.x - v.x, c1 = a.y - v.y, c2 = a.z - v.z, c3 = a.w - v.w;
+    acc[0] = __fmaf_rn(c0, c0, acc[0]);
+    acc[1] = __fmaf_rn(c1, c1, acc[1]);
+    acc[2] = __fmaf_rn(c2, c2, acc[2]);
+    acc[3] = __fmaf_rn(c3, c3, acc[3]);
+  } else {
+    acc[0] = __fmaf_rn(a.x, v.x, acc[0]);
+    acc[1] = __fmaf_rn(a.y, v.y, acc[1]);
+    acc[2] = __fmaf_rn(a.z, v.z, acc[2]);
+    acc[3] = __fmaf_rn(a.w, v.w, acc[3]);
+  }
+}
+
+// Distances of U rows to the shared-memory query `q` (zero padded to a multiple of 8
+// floats) computed by the 8 lanes of a subgroup; rows are padded to 4 floats and 16-byte
+// aligned.  All 8 lanes return the results.  L2, inner product, normalised cosine.
+template <int METRIC, int DIM, int U>
+__device__ __forceinline__ void subgroup_distances(const float* const (&rows)[U],
+                                                   const float* __restrict__ q, uint32_t dim_rt,
+                                                   uint32_t s, unsigned gmask, float (&out)[U]) {
+  const uint32_t dim = DIM > 0 ? (uint32_t)DIM : dim_rt;
+  const uint32_t rem = dim & 7u;
+  const uint32_t full = dim - rem;
+  const float4* q4 = reinterpret_cast<const float4*>(q);
+  float acc[U][4];
+#pragma unroll
+  for (int u = 0; u < U; ++u) acc[u][0] = acc[u][1] = acc[u][2] = acc[u][3] = 0.0f;
+#pragma unroll 4
+  for (uint32_t base = 4u * s; base < full; base += 32u) {
+    const float4 a = q4[base >> 2];
+    float4 v[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) v[u] = __ldg(reinterpret_cast<const float4*>(rows[u]) + (base >> 2));
+#pragma unroll
+    for (int u = 0; u < U; ++u) acc4<METRIC>(a, v[u], acc[u]);
+  }
+#pragma unroll
+  for (int u = 0; u < U; ++u)
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      acc[u][i] += __shfl_xor_sync(gmask, acc[u][i], 2, 8);  // s0+s1 / s2+s3
+      acc[u][i] += __shfl_xor_sync(gmask, acc[u][i], 4, 8);  // (s0+s1)+(s2+s3)
+    }
+  if (rem) {
+    const uint32_t e = full + 4u * (s & 1u);
+    if (e < dim) {
+      const float4 a = q4[e >> 2];
+      const float av[4] = {a.x, a.y, a.z, a.w};
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const float4 v = __ldg(reinterpret_cast<const float4*>(rows[u]) + (e >> 2));
+        const float vv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          if (e + i < dim) {
+            if (METRIC == DK_METRIC_L2) {
+              const float c = av[i] - vv[i];
+              acc[u][i] = __fmaf_rn(c, c, acc[u][i]);
+            } else {
+              acc[u][i] = __fmaf_rn(av[i], vv[i], acc[u][i]);
+            }
+          }
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) acc[u][i] += __shfl_xor_sync(gmask, acc[u][i], 1, 8);
+    const float r = tree4(acc[u][0], acc[u][1], acc[u][2], acc[u][3]);
+    out[u] = METRIC == DK_METRIC_L2 ? r : (METRIC == DK_METRIC_INNER_PRODUCT ? -r : 1.0f - r);
+  }
+}
+
+// Cosine (CosineStateless, simd.rs:2430-2460): three accumulators with the same lane
+// mapping; sum (simd.rs:2327-2361): zero similarity if a norm is below f32::MIN_POSITIVE,
+// else clamp(prod / (sqrt(nx) * sqrt(ny)), -1, 1); distance 1 - similarity.
+template <int DIM>
+__device__ __forceinline__ float subgroup_cosine(const float* __restrict__ row,
+                                                 const float* __restrict__ q, uint32_t dim_rt,
+                                                 uint32_t s, unsigned gmask) {
+  const uint32_t dim = DIM > 0 ? (uint32_t)DIM : dim_rt;
+  const uint32_t rem = dim & 7u;
+  const uint32_t full = dim - rem;
+  const float4* row4 = reinterpret_cast<const float4*>(row);
+  const float4* q4 = reinterpret_cast<const float4*>(q);
+  float xx[4] = {0.f, 0.f, 0.f, 0.f}, yy[4] = {0.f, 0.f, 0.f, 0.f}, xy[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll 4
+  for (uint32_t base = 4u * s; base < full; base += 32u) {
+    const float4 v = __ldg(row4 + (base >> 2));
+    const float4 a = q4[base >> 2];
+    const float av[4] = {a.x, a.y, a.z, a.w}, vv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      xx[i] = __fmaf_rn(av[i], av[i], xx[i]);
+      yy[i] = __fmaf_rn(vv[i], vv[i], yy[i]);
+      xy[i] = __fmaf_rn(av[i], vv[i], xy[i]);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    xx[i] += __shfl_xor_sync(gmask, xx[i], 2, 8);
+    yy[i] += __shfl_xor_sync(gmask, yy[i], 2, 8);
+    xy[i] += __shfl_xor_sync(gmask, xy[i], 2, 8);
+    xx[i] += __shfl_xor_sync(gmask, xx[i], 4, 8);
+    yy[i] += __shfl_xor_sync(gmask, yy[i], 4, 8);
+    xy[i] += __shfl_xor_sync(gmask, xy[i], 4, 8);
+  }
+  if (rem) {
+    const uint32_t e = full + 4u * (s & 1u);
+    if (e < dim) {
+      const float4 v = __ldg(row4 + (e >> 2));
+      const float4 a = q4[e >> 2];
+      const float av[4] = {a.x, a.y, a.z, a.w}, vv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        if (e + i < dim) {
+          xx[i] = __fmaf_rn(av[i], av[i], xx[i]);
+          yy[i] = __fmaf_rn(vv[i], vv[i], yy[i]);
+          xy[i] = __fmaf_rn(av[i], vv[i], xy[i]);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    xx[i] += __shfl_xor_sync(gmask, xx[i], 1, 8);
+    yy[i] += __shfl_xor_sync(gmask, yy[i], 1, 8);
+    xy[i] += __shfl_xor_sync(gmask, xy[i], 1, 8);
+  }
+  const float nx = tree4(xx[0], xx[1], xx[2], xx[3]);
+  const float ny = tree4(yy[0], yy[1], yy[2], yy[3]);
+  const float denom = __fmul_rn(__fsqrt_rn(nx), __fsqrt_rn(ny));
+  const float prod = tree4(xy[0], xy[1], xy[2], xy[3]);
+  float sim;
+  if (nx < 1.17549435e-38f || ny < 1.17549435e-38f) sim = 0.0f;
+  else sim = fmaxf(-1.0f, fminf(1.0f, __fdiv_rn(prod, denom)));
+  return 1.0f - sim;
+}
+
+// Score candidates ids[0..count) into d[...] with subgroup `sg` of `nsub` subgroups; U rows
+// per subgroup are loaded together.  Lanes of a subgroup must be converged.
+template <int METRIC, int DIM, int U>
+__device__ __forceinline__ void score_fp(const SearchParams& P, const float* q,
+                                         const uint32_t* ids, float* d, uint32_t count,
+                                         uint32_t sg, uint32_t nsub, uint32_t s, unsigned gmask) {
+  if (METRIC == DK_METRIC_COSINE) {
+    for (uint32_t i = sg; i < count; i += nsub) {
+      const float r = subgroup_cosine<DIM>(P.vectors + (size_t)ids[i] * P.vstride, q, P.dim, s, gmask);
+      if (s == 0) d[i] = r;
+    }
+    return;
+  }
+  const uint32_t step = nsub * U;
+  for (uint32_t base = 0; base < count; base += step) {
+    const float* rows[U];
+    uint32_t idx[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      idx[u] = base + sg + u * nsub;
+      const uint32_t j = idx[u] < count ? idx[u] : count - 1;  // a valid row; result unused
+      rows[u] = P.vectors + (size_t)ids[j] * P.vstride;
+    }
+    float out[U];
+    subgroup_distances<METRIC, DIM, U>(rows, q, P.dim, s, gmask, out);
+    if (s == 0) {
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        if (idx[u] < count) d[idx[u]] = out[u];
+    }
+  }
+}
+
+// One thread's restatement of the reference kernel for a short slice (PQ chunk distances):
+// same accumulator assignment and reduction, lanes walked serially.
+__device__ __forceinline__ float thread_chunk_distance(const float* __restrict__ x,
+                                                       const float* __restrict__ y, uint32_t len,
+                                                       bool ip) {
+  const uint32_t trip = len / 32u;
+  const uint32_t epi = (len - 32u * trip) / 8u;
+  const uint32_t rem = len & 7u;
+  const uint32_t base = len - rem;
+  float t[8];
+#pragma unroll
+  for (int l = 0; l < 8; ++l) {
+    float s[4] = {0.f, 0.f, 0.f, 0.f};
+    for (uint32_t b = 0; b < trip; ++b) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const uint32_t e = 32u * b + 8u * j + l;
+        if (ip) s[j] = __fmaf_rn(x[e], __ldg(y + e), s[j]);
+        else { const float c = x[e] - __ldg(y + e); s[j] = __fmaf_rn(c, c, s[j]); }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      if ((uint32_t)j < epi) {
+        const uint32_t e = 32u * trip + 8u * j + l;
+        if (ip) s[j] = __fmaf_rn(x[e], __ldg(y + e), s[j]);
+        else { const float c = x[e] - __ldg(y + e); s[j] = __fmaf_rn(c, c, s[j]); }
+      }
+    }
+    float v = (s[0] + s[1]) + (s[2] + s[3]);
+    if ((uint32_t)l < rem) {
+      const uint32_t e = base + l;
+      if (ip) v = __fmaf_rn(x[e], __ldg(y + e), v);
+      else { const float c = x[e] - __ldg(y + e); v = __fmaf_rn(c, c, v); }
+    }
+    t[l] = v;
+  }
+  const float r = tree4(t[0] + t[4], t[1] + t[5], t[2] + t[6], t[3] + t[7]);
+  return ip ? -r : r;
+}
+
+// pq_dist_lookup_single (fixed_chunk_pq_table.rs:79-95): sequential f32 sum, m ascending.
+// The code row's 16-byte words are all loaded before the first lookup.
+__device__ __forceinline__ float pq_distance(const uint8_t* __restrict__ code,
+                                             const float* __restrict__ table, uint32_t m_count) {
+  const uint4* c4 = reinterpret_cast<const uint4*>(code);
+  float acc = 0.0f;
+  if (m_count <= 64) {
+    uint4 w[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+      w[i] = (16u * i < m_count) ? __ldg(c4 + i) : make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll
+    for (uint32_t m = 0; m < 64; ++m) {
+      if (m < m_count) {
+        const uint4 ww = w[m >> 4];
+        const uint32_t word = ((m >> 2) & 3u) == 0 ? ww.x : ((m >> 2) & 3u) == 1 ? ww.y
+                              : ((m >> 2) & 3u) == 2 ? ww.z : ww.w;
+        acc += table[m * 256u + ((word >> (8u * (m & 3u))) & 0xFFu)];
+      }
+    }
+    return acc;
+  }
+  for (uint32_t m0 = 0; m0 < m_count; m0 += 16u) {
+    const uint4 ww = __ldg(c4 + (m0 >> 4));
+    const uint32_t words[4] = {ww.x, ww.y, ww.z, ww.w};
+#pragma unroll
+    for (uint32_t j = 0; j < 16u; ++j)
+      if (m0 + j < m_count)
+        acc += table[(m0 + j) * 256u + ((words[j >> 2] >> (8u * (j & 3u))) & 0xFFu)];
+  }
+  return acc;
+}
+
+// Per-query ADC table (fixed_chunk_pq_table.rs:149-215): L2 table for L2 and
+// CosineNormalized, -dot table for InnerProduct (pq/distance/dynamic.rs:64-84).  Pivots are
+// read chunk-major (chunk m, centre c, len_m floats), so consecutive threads read
+// consecutive 16-byte pieces.
+template <int METRIC>
+__device__ __forceinline__ void build_table(const SearchParams& P, const float* q, float* table,
+                                            uint32_t tid, uint32_t nt) {
+  const bool ip = METRIC == DK_METRIC_INNER_PRODUCT;
+  const uint32_t total = P.pq_chunks * 256u;
+#pragma unroll 4
+  for (uint32_t idx = tid; idx < total; idx += nt) {
+    const uint32_t m = idx >> 8, c = idx & 255u;
+    const uint32_t start = __ldg(P.offsets + m), stop = __ldg(P.offsets + m + 1);
+    const uint32_t len = stop - start;
+    table[idx] = thread_chunk_distance(q + start, P.pivots_cm + (size_t)start * 256u + c * len,
+                                       len, ip);
+  }
+}
+
+// ----------------------------------------------------------------------------------------
+// Shared-memory state of one query (both kernels).
+// ----------------------------------------------------------------------------------------
+
+struct Misc {
+  uint32_t size, cursor, cur, nbeam, nvalid, inserted, overflow, result_count;
+  uint32_t beam[64];
+  uint32_t warp_sums[32];
+};
+
+struct State {
+  float* q;
+  float* table;
+  float* qd[2];
+  uint32_t* qi[2];
+  uint32_t* cand_id;
+  float* cand_d;
+  float* new_d;
+  uint32_t* new_id;
+  uint32_t* hash;
+  Misc* misc;
+};
+
+__device__ __forceinline__ State carve(unsigned char* base, const SearchParams& P) {
+  State S;
+  S.q = reinterpret_cast<float*>(base + P.off_query);
+  S.table = reinterpret_cast<float*>(base + P.off_table);
+  S.qd[0] = reinterpret_cast<float*>(base + P.off_qd0);
+  S.qd[1] = reinterpret_cast<float*>(base + P.off_qd1);
+  S.qi[0] = reinterpret_cast<uint32_t*>(base + P.off_qi0);
+  S.qi[1] = reinterpret_cast<uint32_t*>(base + P.off_qi1);
+  S.cand_id = reinterpret_cast<uint32_t*>(base + P.off_cand_id);
+  S.cand_d = reinterpret_cast<float*>(base + P.off_cand_d);
+  S.new_d = reinterpret_cast<float*>(base + P.off_new_d);
+  S.new_id = reinterpret_cast<uint32_t*>(base + P.off_new_id);
+  S.hash = reinterpret_cast<uint32_t*>(base + P.off_hash);
+  S.misc = reinterpret_cast<Misc*>(base + P.off_misc);
+  return S;
+}
+
+__device__ __forceinline__ void record_hint(const SearchParams& P, uint32_t cmps) {
+  if (P.hint) atomicMax(P.hint, (uint32_t)(((uint64_t)cmps << 8) / P.cap));
+}
+
+// ========================================================================================
+// CTA-per-query kernel.
+// ========================================================================================
+
+template <int NT, int METRIC, bool PQ, int DIM>
+__device__ __forceinline__ void cta_score(const SearchParams& P, const State& S, const uint32_t* ids,
+                                          float* d, uint32_t count) {
+  const uint32_t tid = threadIdx.x;
+  if (PQ) {
+    for (uint32_t i = tid; i < count; i += NT)
+      d[i] = pq_distance(P.codes + (size_t)ids[i] * P.cstride, S.table, P.pq_chunks);
+  } else {
+    const unsigned gmask = 0xFFu << (8u * ((tid & 31u) >> 3));
+    score_fp<METRIC, DIM, 1>(P, S.q, ids, d, count, tid >> 3, NT / 8, tid & 7u, gmask);
+  }
+}
+
+template <int NT>
+__device__ __forceinline__ void cta_merge(const SearchParams& P, const State& S, uint32_t count) {
+  const uint32_t tid = threadIdx.x;
+  Misc* M = S.misc;
+  uint32_t my_valid = 0;
+  for (uint32_t i = tid; i < count; i += NT) {
+    const float d = S.cand_d[i];
+    if (d != d) continue;
+    uint32_t r = 0;
+    for (uint32_t j = 0; j < count; ++j) {
+      const float dj = S.cand_d[j];
+      r += (dj < d) || (dj == d && j > i);
+    }
+    S.new_d[r] = d;
+    S.new_id[r] = S.cand_id[i];
+    ++my_valid;
+  }
+  if (my_valid) atomicAdd(&M->nvalid, my_valid);
+  __syncthreads();
+  const uint32_t nvalid = M->nvalid;
+  const uint32_t size = M->size, cur = M->cur, nxt = cur ^ 1u;
+  const uint32_t cap = P.cap;
+  const uint32_t new_size = min(size + nvalid, cap);
+  const float* od = S.qd[cur];
+  const uint32_t* oi = S.qi[cur];
+  float* wd = S.qd[nxt];
+  uint32_t* wi = S.qi[nxt];
+  for (uint32_t o = tid; o < size; o += NT) {
+    const float d = od[o];
+    const uint32_t pos = o + count_less_equal(S.new_d, nvalid, d);
+    if (pos < cap) { wd[pos] = d; wi[pos] = oi[o]; }
+  }
+  for (uint32_t r = tid; r < nvalid; r += NT) {
+    const float d = S.new_d[r];
+    const uint32_t pos = r + count_less(od, size, d);
+    if (pos < cap) { wd[pos] = d; wi[pos] = S.new_id[r]; }
+  }
+  __syncthreads();
+  if (tid == 0) {
+    const uint32_t c = M->cursor;
+    uint32_t nc = new_size;
+    if (c < size) nc = min(nc, c + count_less_equal(S.new_d, nvalid, od[c]));
+    if (nvalid > 0) nc = min(nc, count_less(od, size, S.new_d[0]));
+    M->cursor = nc;
+    M->size = new_size;
+    M->cur = nxt;
+    M->nvalid = 0;
+  }
+  __syncthreads();
+}
+
+template <int NT, int METRIC, int DIM>
+__device__ void cta_post_process(const SearchParams& P, const State& S, uint32_t qid) {
+  const uint32_t tid = threadIdx.x;
+  Misc* M = S.misc;
+  const uint32_t size = M->size;
+  const float* qd = S.qd[M->cur];
+  const uint32_t* qi = S.qi[M->cur];
+  uint32_t* out_ids = P.out_ids + (size_t)qid * P.k;
+  float* out_d = P.out_dists + (size_t)qid * P.k;
+  uint32_t written;
+  uint32_t base = 0;
+  for (uint32_t t0 = 0; t0 < size; t0 += NT) {
+    const uint32_t i = t0 + tid;
+    const uint32_t id = i < size ? (qi[i] & kIdMask) : 0u;
+    const bool keep = i < size && id < P.n;  // FilterStartPoints (glue.rs:730-773)
+    uint32_t total;
+    const uint32_t pos = base + block_scan<NT>(keep, M->warp_sums, total);
+    if (keep) {
+      if (P.strategy == DK_STRATEGY_HYBRID) S.cand_id[pos] = id;
+      else if (pos < P.k) { out_ids[pos] = id; out_d[pos] = qd[i]; }
+    }
+    base += total;
+  }
+  if (P.strategy != DK_STRATEGY_HYBRID) {
+    written = min(base, P.k);
+  } else {
+    // Rerank (inmem/full_precision.rs:357-404): exact distances, stable sort, first k.
+    const uint32_t count = base;
+    __syncthreads();
+    cta_score<NT, METRIC, false, DIM>(P, S, S.cand_id, S.cand_d, count);
+    __syncthreads();
+    for (uint32_t i = tid; i < count; i += NT) {
+      const float d = S.cand_d[i];
+      const bool dn = d != d;
+      uint32_t r = 0;
+      for (uint32_t j = 0; j < count && r < P.k; ++j) {
+        const float dj = S.cand_d[j];
+        const bool jn = dj != dj;
+        r += dn ? (jn && j < i) : (!jn && (dj < d || (dj == d && j < i)));
+      }
+      if (r < P.k) { out_ids[r] = S.cand_id[i]; out_d[r] = d; }
+    }
+    written = min(count, P.k);
+  }
+  for (uint32_t j = written + tid; j < P.k; j += NT) {
+    out_ids[j] = DK_INVALID_ID;
+    out_d[j] = INFINITY;
+  }
+  if (tid == 0) M->result_count = written;
+}
+
+// The whole search of one query by one CTA.  Returns false if the visited set overflowed.
+template <int NT, int METRIC, bool PQ, int DIM, class VSet>
+__device__ bool cta_search(const SearchParams& P, const State& S, const VSet& vset, uint32_t qid,
+                           uint32_t& cmps_out, uint32_t& hops_out) {
+  const uint32_t tid = threadIdx.x;
+  Misc* M = S.misc;
+  const float* qsrc = P.queries + (size_t)qid * P.qstride;
+  const uint32_t dpad = (P.dim + 7u) & ~7u;
+  for (uint32_t i = tid; i < dpad; i += NT) S.q[i] = i < P.dim ? qsrc[i] : 0.0f;
+  vset.clear(tid, NT);
+  if (tid == 0) {
+    M->size = M->cursor = M->cur = M->inserted = M->overflow = M->nvalid = 0;
+  }
+  __syncthreads();
+  if (PQ) {
+    build_table<METRIC>(P, S.q, S.table, tid, NT);
+    __syncthreads();
+  }
+  if (P.f + P.beam * P.max_degree > P.hash_limit) return false;
+  // Start points (index.rs:1956-1963): visited, scored and inserted in order.
+  for (uint32_t s = tid; s < P.f; s += NT) {
+    S.cand_id[s] = P.n + s;
+    vset.insert(P.n + s);
+  }
+  if (tid == 0) M->inserted = P.f;
+  __syncthreads();
+  cta_score<NT, METRIC, PQ, DIM>(P, S, S.cand_id, S.cand_d, P.f);
+  __syncthreads();
+  cta_merge<NT>(P, S, P.f);
+  uint32_t cmps = P.f, hops = 0;
+  while (true) {
+    if (tid == 0) {  // closest_notvisited x beam (queue.rs:297-313)
+      uint32_t nb = 0, c = M->cursor;
+      const uint32_t size = M->size;
+      uint32_t* qi = S.qi[M->cur];
+      while (nb < P.beam && c < size) {
+        M->beam[nb++] = qi[c] & kIdMask;
+        qi[c] |= kVisited;
+        ++c;
+        while (c < size && (qi[c] & kVisited)) ++c;
+      }
+      M->cursor = c;
+      M->nbeam = nb;
+      if (nb && M->inserted + nb * P.max_degree > P.hash_limit) M->overflow = 1;
+    }
+    __syncthreads();
+    const uint32_t nb = M->nbeam;
+    if (nb == 0) break;
+    if (M->overflow) return false;
+    uint32_t count = 0;
+    for (uint32_t b = 0; b < nb; ++b) {
+      const uint32_t* row = P.adj + (size_t)M->beam[b] * P.astride;
+      const uint32_t deg = __ldg(row);
+      for (uint32_t t0 = 0; t0 < deg; t0 += NT) {
+        const uint32_t t = t0 + tid;
+        bool fresh = false;
+        uint32_t id = 0;
+        if (t < deg) {
+          id = __ldg(row + 1 + t);
+          fresh = vset.insert(id);
+        }
+        uint32_t total;
+        const uint32_t pos = block_scan<NT>(fresh, M->warp_sums, total);
+        if (fresh) S.cand_id[count + pos] = id;
+        count += total;
+      }
+    }
+    if (tid == 0) M->inserted += count;
+    __syncthreads();
+    cta_score<NT, METRIC, PQ, DIM>(P, S, S.cand_id, S.cand_d, count);
+    __syncthreads();
+    cta_merge<NT>(P, S, count);
+    cmps += count;
+    hops += nb;
+  }
+  cmps_out = cmps;
+  hops_out = hops;
+  return true;
+}
+
+template <int NT, int METRIC, bool PQ, int DIM>
+__global__ void __launch_bounds__(NT) k_search_cta(const SearchParams P) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const State S = carve(smem, P);
+  SmemHashSet vset{S.hash, (1u << P.hash_log2) - 1u, 32u - P.hash_log2};
+  const uint32_t qid = blockIdx.x;
+  if (qid >= P.nq) return;
+  uint32_t cmps = 0, hops = 0;
+  if (!cta_search<NT, METRIC, PQ, DIM>(P, S, vset, qid, cmps, hops)) {
+    if (threadIdx.x == 0) P.stats[qid] = dk_search_stats{0u, 0u, 0u, kFlagSpilled};
+    return;
+  }
+  cta_post_process<NT, METRIC, DIM>(P, S, qid);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    P.stats[qid] = dk_search_stats{cmps, hops, S.misc->result_count, 0u};
+    record_hint(P, cmps);
+  }
+}
+
+// Spill pass: each CTA owns one bitmap slice and re-runs the queries the first pass flagged.
+template <int NT, int METRIC, bool PQ, int DIM>
+__global__ void __launch_bounds__(NT) k_search_spill(const SearchParams P) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const State S = carve(smem, P);
+  BitmapSet vset{P.bitmap + (size_t)blockIdx.x * P.bitmap_words, P.bitmap_words};
+  for (uint32_t qid = blockIdx.x; qid < P.nq; qid += gridDim.x) {
+    if (!(P.stats[qid].flags & kFlagSpilled)) continue;
+    __syncthreads();
+    uint32_t cmps = 0, hops = 0;
+    cta_search<NT, METRIC, PQ, DIM>(P, S, vset, qid, cmps, hops);
+    cta_post_process<NT, METRIC, DIM>(P, S, qid);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      P.stats[qid] = dk_search_stats{cmps, hops, S.misc->result_count, kFlagSpilled};
+      record_hint(P, cmps);
+    }
+    __syncthreads();
+  }
+}
+
+// ========================================================================================
+// Warp-per-query kernel.
+// ========================================================================================
+
+// Merge cand_{id,d}[0..count) into the queue; queue bookkeeping lives in registers (the
+// same value in every lane).
+__device__ __forceinline__ void warp_merge(const SearchParams& P, const State& S, uint32_t count,
+                                           uint32_t lane, uint32_t& size, uint32_t& cursor,
+                                           uint32_t& cur) {
+  uint32_t nvalid = 0;
+  for (uint32_t i0 = 0; i0 < count; i0 += 32u) {
+    const uint32_t i = i0 + lane;
+    const float d = i < count ? S.cand_d[i] : 0.0f;
+    const bool valid = i < count && d == d;
+    if (valid) {
+      uint32_t r = 0;
+      for (uint32_t j = 0; j < count; ++j) {
+        const float dj = S.cand_d[j];
+        r += (dj < d) || (dj == d && j > i);
+      }
+      S.new_d[r] = d;
+      S.new_id[r] = S.cand_id[i];
+    }
+    nvalid += __popc(__ballot_sync(kFull, valid));
+  }
+  __syncwarp();
+  const uint32_t cap = P.cap, nxt = cur ^ 1u;
+  const uint32_t new_size = min(size + nvalid, cap);
+  const float* od = S.qd[cur];
+  const uint32_t* oi = S.qi[cur];
+  float* wd = S.qd[nxt];
+  uint32_t* wi = S.qi[nxt];
+  for (uint32_t o = lane; o < size; o += 32u) {
+    const float d = od[o];
+    const uint32_t pos = o + count_less_equal(S.new_d, nvalid, d);
+    if (pos < cap) { wd[pos] = d; wi[pos] = oi[o]; }
+  }
+  for (uint32_t r = lane; r < nvalid; r += 32u) {
+    const float d = S.new_d[r];
+    const uint32_t pos = r + count_less(od, size, d);
+    if (pos < cap) { wd[pos] = d; wi[pos] = S.new_id[r]; }
+  }
+  uint32_t nc = new_size;
+  if (cursor < size) nc = min(nc, cursor + count_less_equal(S.new_d, nvalid, od[cursor]));
+  if (nvalid > 0) nc = min(nc, count_less(od, size, S.new_d[0]));
+  cursor = nc;
+  size = new_size;
+  cur = nxt;
+  __syncwarp();
+}
+
+template <int METRIC, bool PQ, int DIM, int U>
+__device__ __forceinline__ void warp_score(const SearchParams& P, const State& S,
+                                           const uint32_t* ids, float* d, uint32_t count,
+                                           uint32_t lane) {
+  if (PQ) {
+    for (uint32_t i = lane; i < count; i += 32u)
+      d[i] = pq_distance(P.codes + (size_t)ids[i] * P.cstride, S.table, P.pq_chunks);
+  } else {
+    const unsigned gmask = 0xFFu << (8u * (lane >> 3));
+    score_fp<METRIC, DIM, U>(P, S.q, ids, d, count, lane >> 3, 4u, lane & 7u, gmask);
+  }
+  __syncwarp();
+}
+
+template <int METRIC, int DIM, int U>
+__device__ void warp_post_process(const SearchParams& P, const State& S, uint32_t qid,
+                                  uint32_t lane, uint32_t size, uint32_t cur,
+                                  uint32_t& result_count) {
+  const float* qd = S.qd[cur];
+  const uint32_t* qi = S.qi[cur];
+  uint32_t* out_ids = P.out_ids + (size_t)qid * P.k;
+  float* out_d = P.out_dists + (size_t)qid * P.k;
+  const bool hybrid = P.strategy == DK_STRATEGY_HYBRID;
+  uint32_t base = 0;
+  for (uint32_t t0 = 0; t0 < size; t0 += 32u) {
+    if (!hybrid && base >= P.k) break;
+    const uint32_t i = t0 + lane;
+    const uint32_t id = i < size ? (qi[i] & kIdMask) : 0u;
+    const bool keep = i < size && id < P.n;  // FilterStartPoints (glue.rs:730-773)
+    const uint32_t m = __ballot_sync(kFull, keep);
+    const uint32_t pos = base + __popc(m & lanemask_lt());
+    if (keep) {
+      if (hybrid) S.cand_id[pos] = id;
+      else if (pos < P.k) { out_ids[pos] = id; out_d[pos] = qd[i]; }
+    }
+    base += __popc(m);
+  }
+  uint32_t written;
+  if (!hybrid) {
+    written = min(base, P.k);
+  } else {
+    // Rerank (inmem/full_precision.rs:357-404): exact distances, stable sort, first k.
+    const uint32_t count = base;
+    __syncwarp();
+    warp_score<METRIC, false, DIM, U>(P, S, S.cand_id, S.cand_d, count, lane);
+    for (uint32_t i = lane; i < count; i += 32u) {
+      const float d = S.cand_d[i];
+      const bool dn = d != d;
+      uint32_t r = 0;
+      for (uint32_t j = 0; j < count && r < P.k; ++j) {
+        const float dj = S.cand_d[j];
+        const bool jn = dj != dj;
+        r += dn ? (jn && j < i) : (!jn && (dj < d || (dj == d && j < i)));
+      }
+      if (r < P.k) { out_ids[r] = S.cand_id[i]; out_d[r] = d; }
+    }
+    written = min(count, P.k);
+  }
+  for (uint32_t j = written + lane; j < P.k; j += 32u) {
+    out_ids[j] = DK_INVALID_ID;
+    out_d[j] = INFINITY;
+  }
+  result_count = written;
+}
+
+template <int METRIC, bool PQ, int DIM, int U>
+__global__ void __launch_bounds__(128) k_search_warp(const SearchParams P) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  const uint32_t qid = blockIdx.x * (blockDim.x >> 5) + warp;
+  if (qid >= P.nq) return;  // whole warp; no block-level synchronisation below
+  const State S = carve(smem + (size_t)warp * P.warp_smem, P);
+  const SmemHashSet vset{S.hash, (1u << P.hash_log2) - 1u, 32u - P.hash_log2};
+
+  const float* qsrc = P.queries + (size_t)qid * P.qstride;
+  const uint32_t dpad = (P.dim + 7u) & ~7u;
+  for (uint32_t i = lane; i < dpad; i += 32u) S.q[i] = i < P.dim ? qsrc[i] : 0.0f;
+  vset.clear(lane, 32u);
+  __syncwarp();
+  if (PQ) {
+    build_table<METRIC>(P, S.q, S.table, lane, 32u);
+    __syncwarp();
+  }
+  if (P.f + P.beam * P.max_degree > P.hash_limit) {
+    if (lane == 0) P.stats[qid] = dk_search_stats{0u, 0u, 0u, kFlagSpilled};
+    return;
+  }
+  uint32_t size = 0, cursor = 0, cur = 0, inserted = P.f;
+  for (uint32_t s = lane; s < P.f; s += 32u) {
+    S.cand_id[s] = P.n + s;
+    vset.insert(P.n + s);
+  }
+  __syncwarp();
+  warp_score<METRIC, PQ, DIM, U>(P, S, S.cand_id, S.cand_d, P.f, lane);
+  warp_merge(P, S, P.f, lane, size, cursor, cur);
+  uint32_t cmps = P.f, hops = 0;
+  uint32_t* beam = S.misc->beam;
+
+  while (cursor < size) {
+    // closest_notvisited x beam (queue.rs:297-313); `cursor` is the first unvisited entry.
+    uint32_t nb = 0, c = cursor;
+    uint32_t* qi = S.qi[cur];
+    while (c < size) {
+      const uint32_t idx = c + lane;
+      const bool unv = idx < size && !(qi[idx] & kVisited);
+      uint32_t m = __ballot_sync(kFull, unv);
+      if (nb < P.beam) {
+        const uint32_t take = min((uint32_t)__popc(m), P.beam - nb);
+        const uint32_t rank = __popc(m & lanemask_lt());
+        if (unv && rank < take) {
+          beam[nb + rank] = qi[idx] & kIdMask;
+          qi[idx] |= kVisited;
+        }
+        nb += take;
+        for (uint32_t t = 0; t < take; ++t) m &= m - 1u;
+      }
+      if (m) {
+        c += __ffs(m) - 1u;
+        break;
+      }
+      c += 32u;
+    }
+    cursor = min(c, size);
+    __syncwarp();
+    if (inserted + nb * P.max_degree > P.hash_limit) {
+      if (lane == 0) P.stats[qid] = dk_search_stats{0u, 0u, 0u, kFlagSpilled};
+      return;
+    }
+    // Expand: adjacency rows in beam order, ids through the visited set in order.
+    uint32_t count = 0;
+    for (uint32_t b = 0; b < nb; ++b) {
+      const uint32_t* row = P.adj + (size_t)beam[b] * P.astride;
+      const uint32_t deg = __ldg(row);
+      uint32_t ids[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const uint32_t t = 32u * r + lane;
+        ids[r] = t < P.max_degree ? __ldg(row + 1 + t) : 0u;
+      }
+      for (uint32_t t0 = 0; t0 < deg; t0 += 32u) {
+        const uint32_t t = t0 + lane;
+        uint32_t id;
+        if (t0 < 128u) {
+          const uint32_t r = t0 >> 5;
+          id = r == 0 ? ids[0] : r == 1 ? ids[1] : r == 2 ? ids[2] : ids[3];
+        } else {
+          id = t < deg ? __ldg(row + 1 + t) : 0u;
+        }
+        const bool fresh = t < deg && vset.insert(id);
+        const uint32_t m = __ballot_sync(kFull, fresh);
+        if (fresh) S.cand_id[count + __popc(m & lanemask_lt())] = id;
+        count += __popc(m);
+      }
+    }
+    inserted += count;
+    __syncwarp();
+    warp_score<METRIC, PQ, DIM, U>(P, S, S.cand_id, S.cand_d, count, lane);
+    warp_merge(P, S, count, lane, size, cursor, cur);
+    cmps += count;
+    hops += nb;
+  }
+  uint32_t result_count = 0;
+  warp_post_process<METRIC, DIM, U>(P, S, qid, lane, size, cur, result_count);
+  if (lane == 0) {
+    P.stats[qid] = dk_search_stats{cmps, hops, result_count, 0u};
+    record_hint(P, cmps);
+  }
+}
+
+// ========================================================================================
+// Launch helpers (host).
+// ========================================================================================
+
+enum class KernelKind { kWarp, kCta };
+
+struct LaunchPlan {
+  SearchParams p1;     // first pass (warp or CTA layout, with hash)
+  SearchParams p2;     // spill pass (CTA layout, bitmap)
+  KernelKind kind;
+  uint32_t warps_per_cta;
+  uint32_t spill_ctas;
+  uint32_t launches;   // kernels launched (reported to callers that count them)
+};
+
+template <int METRIC, bool PQ, int DIM>
+cudaError_t launch_variant(const LaunchPlan& L, cudaStream_t stream) {
+  cudaError_t e;
+  constexpr int U = (DIM > 0 && DIM <= 128) ? 2 : 1;
+  if (L.kind == KernelKind::kWarp) {
+    auto k1 = k_search_warp<METRIC, PQ, DIM, U>;
+    const uint32_t bytes = L.p1.warp_smem * L.warps_per_cta;
+    e = cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) return e;
+    const uint32_t grid = (L.p1.nq + L.warps_per_cta - 1) / L.warps_per_cta;
+    k1<<<grid, 32 * L.warps_per_cta, bytes, stream>>>(L.p1);
+  } else {
+    auto k1 = k_search_cta<kCtaThreads, METRIC, PQ, DIM>;
+    e = cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.p1.smem_bytes);
+    if (e != cudaSuccess) return e;
+    k1<<<L.p1.nq, kCtaThreads, L.p1.smem_bytes, stream>>>(L.p1);
+  }
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  auto k2 = k_search_spill<kCtaThreads, METRIC, PQ, DIM>;
+  e = cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.p2.smem_bytes);
+  if (e != cudaSuccess) return e;
+  k2<<<L.spill_ctas, kCtaThreads, L.p2.smem_bytes, stream>>>(L.p2);
+  return cudaGetLastError();
+}
+
+template <int METRIC, bool PQ>
+cudaError_t launch_dims(const LaunchPlan& L, cudaStream_t stream) {
+  switch (L.p1.dim) {
+    case 96: return launch_variant<METRIC, PQ, 96>(L, stream);
+    case 128: return launch_variant<METRIC, PQ, 128>(L, stream);
+    case 384: return launch_variant<METRIC, PQ, 384>(L, stream);
+    case 768: return launch_variant<METRIC, PQ, 768>(L, stream);
+    default: return launch_variant<METRIC, PQ, 0>(L, stream);
+  }
+}
+
+}  // namespace dk
+
+// Per-metric entry points (one translation unit each, compiled in parallel).
+cudaError_t dk_launch_l2(const dk::LaunchPlan& L, bool pq, cudaStream_t stream);
+cudaError_t dk_launch_ip(const dk::LaunchPlan& L, bool pq, cudaStream_t stream);
+cudaError_t dk_launch_cosine(const dk::LaunchPlan& L, bool pq, cudaStream_t stream);
+cudaError_t dk_launch_cosine_normalized(const dk::LaunchPlan& L, bool pq, cudaStream_t stream);

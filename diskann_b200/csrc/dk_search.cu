@@ -1,676 +1,23 @@
-// Batched greedy beam search on B200 (sm_100a).
-//
-// One CTA runs one query's whole `search_internal` loop (diskann/src/graph/index.rs:
-// 1938-2005) with its state resident in shared memory:
-//   * the candidate queue (diskann/src/neighbor/queue.rs:68-519): two sorted arrays of
-//     (distance, id|visited-bit) with capacity L + #start points, double-buffered so a hop's
-//     new candidates are merged in one parallel pass;
-//   * the visited set (diskann/src/graph/search/scratch.rs:41-48, glue.rs:524-561): an
-//     open-addressing u32 hash; a query that would load it past its limit is re-run in a
-//     spill pass with an exact per-CTA bitmap over all ids in global memory;
-//   * the query vector and, for PQ traversal, the per-query ADC table
-//     (diskann-providers/src/model/pq/fixed_chunk_pq_table.rs:149-215).
-//
-// Per hop: pop the beam from the queue cursor; read each beam node's adjacency row (one
-// contiguous HBM row per node); filter ids through the visited set in adjacency order
-// (block-wide ballot compaction keeps the reference's order); score the new ids; merge.
-//
-// Scoring full-precision candidates uses 8-lane subgroups: lane s of a subgroup reads
-// 16-byte float4 pieces at offsets 32*b + 4*s of the row, which makes lane s own exactly the
-// accumulator lanes 4s..4s+3 of the reference's x86-64-v3 kernel (four f32x8 accumulators
-// over 32-float blocks, diskann-vector/src/distance/simd.rs:321-363, 686-745), so the
-// reduction below reproduces the reference's float rounding sequence bit for bit:
-// (s0+s1)+(s2+s3) lane-wise, masked remainder, then sum_tree
-// (diskann-wide/src/arch/x86_64/v3/f32x8_.rs:187-212).
-//
-// Merge semantics: the reference inserts a hop's candidates one by one in adjacency order;
-// `insert` places an item before existing equal distances (lower bound, queue.rs:130-171),
-// drops it if the queue is full and its distance exceeds the last, and evicts the last
-// otherwise.  That equals keeping the first `cap` entries of the union ordered by
-// (distance, newest first), which is what the merge computes: new items are ranked among
-// themselves by (distance ascending, adjacency position descending) and placed before old
-// items of equal distance.  NaN distances are scored and counted but never inserted.
+// Host side of the batched search: shared-memory planning, visited-set sizing, kernel choice
+// and the two-pass launch (first pass with a shared-memory hash, spill pass with a bitmap).
+// Device code is in dk_kernels.cuh; per-metric instantiations in dk_search_<metric>.cu.
 
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <cmath>
 #include <cstdint>
 #include <cstdlib>
+#include <cstring>
+#include <string>
 
-#include "dk_internal.cuh"
+#include "dk_kernels.cuh"
 
 namespace {
 
-constexpr uint32_t kEmpty = 0xFFFFFFFFu;
-constexpr uint32_t kVisited = 0x80000000u;
-constexpr uint32_t kIdMask = 0x7FFFFFFFu;
-
-// ----------------------------------------------------------------------------------------
-// Visited sets.
-// ----------------------------------------------------------------------------------------
-
-struct SmemHashSet {
-  uint32_t* slots;
-  uint32_t mask;
-  uint32_t shift;
-
-  __device__ void clear(uint32_t tid, uint32_t nt) const {
-    for (uint32_t i = tid; i <= mask; i += nt) slots[i] = kEmpty;
-  }
-  // Returns true if `id` was not present (and is now).  Callers keep the load below the
-  // table size, so the probe always ends.
-  __device__ bool insert(uint32_t id) const {
-    volatile uint32_t* s = slots;
-    uint32_t h = (id * 2654435761u) >> shift;
-    while (true) {
-      const uint32_t cur = s[h];
-      if (cur == id) return false;
-      if (cur == kEmpty) {
-        const uint32_t old = atomicCAS(&slots[h], kEmpty, id);
-        if (old == kEmpty) return true;
-        if (old == id) return false;
-      }
-      h = (h + 1) & mask;
-    }
-  }
-};
-
-struct BitmapSet {
-  uint32_t* words;
-  uint32_t nwords;
-
-  __device__ void clear(uint32_t tid, uint32_t nt) const {
-    for (uint32_t i = tid; i < nwords; i += nt) words[i] = 0u;
-  }
-  __device__ bool insert(uint32_t id) const {
-    const uint32_t bit = 1u << (id & 31u);
-    const uint32_t old = atomicOr(&words[id >> 5], bit);
-    return (old & bit) == 0u;
-  }
-};
-
-// ----------------------------------------------------------------------------------------
-// Block helpers.
-// ----------------------------------------------------------------------------------------
-
-// Exclusive prefix of a 0/1 flag over the block, in thread order; `total` = block sum.
-// Every thread of the block must call it.
-template <int NT>
-__device__ __forceinline__ uint32_t block_scan(bool flag, uint32_t* warp_sums, uint32_t& total) {
-  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-  const uint32_t b = __ballot_sync(0xFFFFFFFFu, flag);
-  const uint32_t pre = __popc(b & ((1u << lane) - 1u));
-  if (lane == 0) warp_sums[warp] = __popc(b);
-  __syncthreads();
-  uint32_t base = 0, tot = 0;
-#pragma unroll
-  for (int w = 0; w < NT / 32; ++w) {
-    const uint32_t s = warp_sums[w];
-    base += (w < (int)warp) ? s : 0u;
-    tot += s;
-  }
-  __syncthreads();
-  total = tot;
-  return base + pre;
-}
-
-// Number of entries of sorted `a[0..n)` that are < d (lower bound) / <= d (upper bound).
-__device__ __forceinline__ uint32_t count_less(const float* a, uint32_t n, float d) {
-  uint32_t lo = 0, hi = n;
-  while (lo < hi) {
-    const uint32_t mid = (lo + hi) >> 1;
-    if (a[mid] < d) lo = mid + 1; else hi = mid;
-  }
-  return lo;
-}
-__device__ __forceinline__ uint32_t count_less_equal(const float* a, uint32_t n, float d) {
-  uint32_t lo = 0, hi = n;
-  while (lo < hi) {
-    const uint32_t mid = (lo + hi) >> 1;
-    if (a[mid] <= d) lo = mid + 1; else hi = mid;
-  }
-  return lo;
-}
-
-// ----------------------------------------------------------------------------------------
-// Distances.
-// ----------------------------------------------------------------------------------------
-
-__device__ __forceinline__ float sum_tree8_lane(float u0, float u1, float u2, float u3) {
-  // After the xor-1 step each lane holds q_i = t_i + t_{i+4} (i = 0..3).
-  const float d0 = u0 + u2, d1 = u1 + u3;
-  return d0 + d1;
-}
-
-// Full-precision distance between the shared-memory query `q` (zero padded to a multiple of
-// 8 floats) and global row `row` (padded to a multiple of 4 floats, 16-B aligned), computed
-// by the 8 lanes of a subgroup; all 8 lanes return the result.  `gmask` = subgroup lanes.
-template <int METRIC, int DIM>
-__device__ __forceinline__ float subgroup_distance(const float* __restrict__ row,
-                                                   const float* __restrict__ q, uint32_t dim_rt,
-                                                   uint32_t s, unsigned gmask) {
-  const uint32_t dim = DIM > 0 ? (uint32_t)DIM : dim_rt;
-  const uint32_t rem = dim & 7u;
-  const uint32_t full = dim - rem;
-  const float4* row4 = reinterpret_cast<const float4*>(row);
-  const float4* q4 = reinterpret_cast<const float4*>(q);
-  if (METRIC == DK_METRIC_COSINE) {
-    float xx[4] = {0.f, 0.f, 0.f, 0.f}, yy[4] = {0.f, 0.f, 0.f, 0.f}, xy[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll 4
-    for (uint32_t base = 4u * s; base < full; base += 32u) {
-      const float4 v = __ldg(row4 + (base >> 2));
-      const float4 a = q4[base >> 2];
-      const float av[4] = {a.x, a.y, a.z, a.w}, vv[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        xx[i] = __fmaf_rn(av[i], av[i], xx[i]);
-        yy[i] = __fmaf_rn(vv[i], vv[i], yy[i]);
-        xy[i] = __fmaf_rn(av[i], vv[i], xy[i]);
-      }
-    }
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      xx[i] += __shfl_xor_sync(gmask, xx[i], 2, 8);
-      yy[i] += __shfl_xor_sync(gmask, yy[i], 2, 8);
-      xy[i] += __shfl_xor_sync(gmask, xy[i], 2, 8);
-      xx[i] += __shfl_xor_sync(gmask, xx[i], 4, 8);
-      yy[i] += __shfl_xor_sync(gmask, yy[i], 4, 8);
-      xy[i] += __shfl_xor_sync(gmask, xy[i], 4, 8);
-    }
-    if (rem) {
-      const uint32_t e = full + 4u * (s & 1u);
-      if (e < dim) {
-        const float4 v = __ldg(row4 + (e >> 2));
-        const float4 a = q4[e >> 2];
-        const float av[4] = {a.x, a.y, a.z, a.w}, vv[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          if (e + i < dim) {
-            xx[i] = __fmaf_rn(av[i], av[i], xx[i]);
-            yy[i] = __fmaf_rn(vv[i], vv[i], yy[i]);
-            xy[i] = __fmaf_rn(av[i], vv[i], xy[i]);
-          }
-        }
-      }
-    }
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      xx[i] += __shfl_xor_sync(gmask, xx[i], 1, 8);
-      yy[i] += __shfl_xor_sync(gmask, yy[i], 1, 8);
-      xy[i] += __shfl_xor_sync(gmask, xy[i], 1, 8);
-    }
-    const float nx = sum_tree8_lane(xx[0], xx[1], xx[2], xx[3]);
-    const float ny = sum_tree8_lane(yy[0], yy[1], yy[2], yy[3]);
-    const float denom = __fmul_rn(__fsqrt_rn(nx), __fsqrt_rn(ny));
-    const float prod = sum_tree8_lane(xy[0], xy[1], xy[2], xy[3]);
-    float sim;
-    if (nx < 1.17549435e-38f || ny < 1.17549435e-38f) {
-      sim = 0.0f;
-    } else {
-      sim = fmaxf(-1.0f, fminf(1.0f, __fdiv_rn(prod, denom)));
-    }
-    return 1.0f - sim;
-  } else {
-    float acc[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll 4
-    for (uint32_t base = 4u * s; base < full; base += 32u) {
-      const float4 v = __ldg(row4 + (base >> 2));
-      const float4 a = q4[base >> 2];
-      if (METRIC == DK_METRIC_L2) {
-        const float c0 = a.x - v.x, c1 = a.y - v.y, c2 = a.z - v.z, c3 = a.w - v.w;
-        acc[0] = __fmaf_rn(c0, c0, acc[0]);
-        acc[1] = __fmaf_rn(c1, c1, acc[1]);
-        acc[2] = __fmaf_rn(c2, c2, acc[2]);
-        acc[3] = __fmaf_rn(c3, c3, acc[3]);
-      } else {
-        acc[0] = __fmaf_rn(a.x, v.x, acc[0]);
-        acc[1] = __fmaf_rn(a.y, v.y, acc[1]);
-        acc[2] = __fmaf_rn(a.z, v.z, acc[2]);
-        acc[3] = __fmaf_rn(a.w, v.w, acc[3]);
-      }
-    }
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      acc[i] += __shfl_xor_sync(gmask, acc[i], 2, 8);  // s0+s1 (lanes 0,1) / s2+s3 (lanes 4,5)
-      acc[i] += __shfl_xor_sync(gmask, acc[i], 4, 8);  // (s0+s1)+(s2+s3)
-    }
-    if (rem) {
-      const uint32_t e = full + 4u * (s & 1u);
-      if (e < dim) {
-        const float4 v = __ldg(row4 + (e >> 2));
-        const float4 a = q4[e >> 2];
-        const float av[4] = {a.x, a.y, a.z, a.w}, vv[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          if (e + i < dim) {
-            if (METRIC == DK_METRIC_L2) {
-              const float c = av[i] - vv[i];
-              acc[i] = __fmaf_rn(c, c, acc[i]);
-            } else {
-              acc[i] = __fmaf_rn(av[i], vv[i], acc[i]);
-            }
-          }
-        }
-      }
-    }
-#pragma unroll
-    for (int i = 0; i < 4; ++i) acc[i] += __shfl_xor_sync(gmask, acc[i], 1, 8);
-    const float r = sum_tree8_lane(acc[0], acc[1], acc[2], acc[3]);
-    if (METRIC == DK_METRIC_L2) return r;
-    if (METRIC == DK_METRIC_INNER_PRODUCT) return -r;
-    return 1.0f - r;  // CosineNormalized
-  }
-}
-
-// One thread's restatement of the reference kernel for a short slice (PQ chunk distances):
-// same accumulator assignment and reduction as above, lanes walked serially.
-__device__ float thread_chunk_distance(const float* __restrict__ x, const float* __restrict__ y,
-                                       uint32_t len, bool ip) {
-  const uint32_t trip = len / 32u;
-  const uint32_t epi = (len - 32u * trip) / 8u;
-  const uint32_t rem = len & 7u;
-  const uint32_t base = len - rem;
-  float t[8];
-#pragma unroll
-  for (int l = 0; l < 8; ++l) {
-    float s[4] = {0.f, 0.f, 0.f, 0.f};
-    for (uint32_t b = 0; b < trip; ++b) {
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const uint32_t e = 32u * b + 8u * j + l;
-        if (ip) s[j] = __fmaf_rn(x[e], __ldg(y + e), s[j]);
-        else { const float c = x[e] - __ldg(y + e); s[j] = __fmaf_rn(c, c, s[j]); }
-      }
-    }
-#pragma unroll
-    for (int j = 0; j < 3; ++j) {
-      if ((uint32_t)j < epi) {
-        const uint32_t e = 32u * trip + 8u * j + l;
-        if (ip) s[j] = __fmaf_rn(x[e], __ldg(y + e), s[j]);
-        else { const float c = x[e] - __ldg(y + e); s[j] = __fmaf_rn(c, c, s[j]); }
-      }
-    }
-    float v = (s[0] + s[1]) + (s[2] + s[3]);
-    if ((uint32_t)l < rem) {
-      const uint32_t e = base + l;
-      if (ip) v = __fmaf_rn(x[e], __ldg(y + e), v);
-      else { const float c = x[e] - __ldg(y + e); v = __fmaf_rn(c, c, v); }
-    }
-    t[l] = v;
-  }
-  const float q0 = t[0] + t[4], q1 = t[1] + t[5], q2 = t[2] + t[6], q3 = t[3] + t[7];
-  const float r = sum_tree8_lane(q0, q1, q2, q3);
-  return ip ? -r : r;
-}
-
-// pq_dist_lookup_single (fixed_chunk_pq_table.rs:79-95): sequential f32 sum, m ascending.
-__device__ __forceinline__ float pq_distance(const uint8_t* __restrict__ code,
-                                             const float* __restrict__ table, uint32_t m_count) {
-  float acc = 0.0f;
-  const uint4* c4 = reinterpret_cast<const uint4*>(code);
-  for (uint32_t m0 = 0; m0 < m_count; m0 += 16u) {
-    const uint4 w = __ldg(c4 + (m0 >> 4));
-    const uint32_t words[4] = {w.x, w.y, w.z, w.w};
-#pragma unroll
-    for (uint32_t j = 0; j < 16u; ++j) {
-      if (m0 + j < m_count) {
-        const uint32_t byte = (words[j >> 2] >> (8u * (j & 3u))) & 0xFFu;
-        acc += table[(m0 + j) * 256u + byte];
-      }
-    }
-  }
-  return acc;
-}
-
-// ----------------------------------------------------------------------------------------
-// Shared-memory state of one query.
-// ----------------------------------------------------------------------------------------
-
-struct Misc {
-  uint32_t size;      // queue size
-  uint32_t cursor;    // first unvisited entry
-  uint32_t cur;       // which queue buffer is current
-  uint32_t nbeam;
-  uint32_t nvalid;    // non-NaN candidates of the batch being merged
-  uint32_t inserted;  // visited-set inserts so far
-  uint32_t overflow;
-  uint32_t pad;
-  uint32_t beam[64];
-  uint32_t warp_sums[32];
-};
-
-struct State {
-  float* q;
-  float* table;
-  float* qd[2];
-  uint32_t* qi[2];
-  uint32_t* cand_id;
-  float* cand_d;
-  float* new_d;
-  uint32_t* new_id;
-  Misc* misc;
-};
-
-__device__ __forceinline__ State carve(unsigned char* smem, const SearchParams& P) {
-  State S;
-  S.q = reinterpret_cast<float*>(smem + P.off_query);
-  S.table = reinterpret_cast<float*>(smem + P.off_table);
-  S.qd[0] = reinterpret_cast<float*>(smem + P.off_qd0);
-  S.qd[1] = reinterpret_cast<float*>(smem + P.off_qd1);
-  S.qi[0] = reinterpret_cast<uint32_t*>(smem + P.off_qi0);
-  S.qi[1] = reinterpret_cast<uint32_t*>(smem + P.off_qi1);
-  S.cand_id = reinterpret_cast<uint32_t*>(smem + P.off_cand_id);
-  S.cand_d = reinterpret_cast<float*>(smem + P.off_cand_d);
-  S.new_d = reinterpret_cast<float*>(smem + P.off_new_d);
-  S.new_id = reinterpret_cast<uint32_t*>(smem + P.off_new_id);
-  S.misc = reinterpret_cast<Misc*>(smem + P.off_misc);
-  return S;
-}
-
-// Score cand_id[0..count) into cand_d (full precision or PQ).
-template <int NT, int METRIC, bool PQ, int DIM>
-__device__ __forceinline__ void score_candidates(const SearchParams& P, const State& S,
-                                                 uint32_t count) {
-  const uint32_t tid = threadIdx.x;
-  if (PQ) {
-    for (uint32_t i = tid; i < count; i += NT) {
-      const uint32_t id = S.cand_id[i];
-      S.cand_d[i] = pq_distance(P.codes + (size_t)id * P.cstride, S.table, P.pq_chunks);
-    }
-  } else {
-    constexpr uint32_t kSub = NT / 8;
-    const uint32_t sg = tid >> 3, s = tid & 7u;
-    const unsigned gmask = 0xFFu << (8u * ((tid & 31u) >> 3));
-    for (uint32_t i = sg; i < count; i += kSub) {
-      const uint32_t id = S.cand_id[i];
-      const float d = subgroup_distance<METRIC, DIM>(P.vectors + (size_t)id * P.vstride, S.q,
-                                                     P.dim, s, gmask);
-      if (s == 0) S.cand_d[i] = d;
-    }
-  }
-}
-
-// Merge the scored batch cand_{id,d}[0..count) into the queue (see file comment).
-template <int NT>
-__device__ __forceinline__ void merge_batch(const SearchParams& P, const State& S, uint32_t count) {
-  const uint32_t tid = threadIdx.x;
-  Misc* M = S.misc;
-  if (tid == 0) M->nvalid = 0;
-  __syncthreads();
-  // Rank new items: (distance ascending, adjacency position descending).
-  uint32_t my_valid = 0;
-  for (uint32_t i = tid; i < count; i += NT) {
-    const float d = S.cand_d[i];
-    if (d != d) continue;  // NaN: never inserted (queue.rs:131-135)
-    uint32_t r = 0;
-    for (uint32_t j = 0; j < count; ++j) {
-      const float dj = S.cand_d[j];
-      r += (dj < d) || (dj == d && j > i);
-    }
-    S.new_d[r] = d;
-    S.new_id[r] = S.cand_id[i];
-    ++my_valid;
-  }
-  if (my_valid) atomicAdd(&M->nvalid, my_valid);
-  __syncthreads();
-  const uint32_t nv = M->nvalid;
-  const uint32_t size = M->size, cur = M->cur, nxt = cur ^ 1u;
-  const uint32_t cap = P.cap;
-  const uint32_t new_size = min(size + nv, cap);
-  const float* od = S.qd[cur];
-  const uint32_t* oi = S.qi[cur];
-  float* wd = S.qd[nxt];
-  uint32_t* wi = S.qi[nxt];
-  for (uint32_t o = tid; o < size; o += NT) {
-    const float d = od[o];
-    const uint32_t pos = o + count_less_equal(S.new_d, nv, d);
-    if (pos < cap) { wd[pos] = d; wi[pos] = oi[o]; }
-  }
-  for (uint32_t r = tid; r < nv; r += NT) {
-    const float d = S.new_d[r];
-    const uint32_t pos = r + count_less(od, size, d);
-    if (pos < cap) { wd[pos] = d; wi[pos] = S.new_id[r]; }
-  }
-  if (tid == 0) {
-    const uint32_t c = M->cursor;
-    uint32_t nc = new_size;
-    if (c < size) nc = min(nc, c + count_less_equal(S.new_d, nv, od[c]));
-    if (nv > 0) nc = min(nc, count_less(od, size, S.new_d[0]));
-    M->cursor = nc;
-    M->size = new_size;
-    M->cur = nxt;
-  }
-  __syncthreads();
-}
-
-// Build the per-query ADC table in shared memory (fixed_chunk_pq_table.rs:149-215; L2 table
-// for L2 and CosineNormalized, -dot table for InnerProduct, pq/distance/dynamic.rs:64-84).
-template <int NT, int METRIC>
-__device__ __forceinline__ void build_table(const SearchParams& P, const State& S) {
-  const bool ip = METRIC == DK_METRIC_INNER_PRODUCT;
-  const uint32_t total = P.pq_chunks * 256u;
-  for (uint32_t idx = threadIdx.x; idx < total; idx += NT) {
-    const uint32_t m = idx >> 8, c = idx & 255u;
-    const uint32_t start = __ldg(P.offsets + m), stop = __ldg(P.offsets + m + 1);
-    S.table[idx] = thread_chunk_distance(S.q + start, P.pivots + (size_t)c * P.dim + start,
-                                         stop - start, ip);
-  }
-}
-
-// Post-processing: FilterStartPoints then copy (FullPrecision, Quantized) or Rerank (Hybrid).
-template <int NT, int METRIC, int DIM>
-__device__ void post_process(const SearchParams& P, const State& S, uint32_t qid) {
-  const uint32_t tid = threadIdx.x;
-  Misc* M = S.misc;
-  const uint32_t size = M->size;  // <= cap = search_l, so all entries are candidates
-  const uint32_t cur = M->cur;
-  const float* qd = S.qd[cur];
-  const uint32_t* qi = S.qi[cur];
-  uint32_t* out_ids = P.out_ids + (size_t)qid * P.k;
-  float* out_d = P.out_dists + (size_t)qid * P.k;
-  uint32_t written = 0;
-  if (P.strategy != DK_STRATEGY_HYBRID) {
-    uint32_t base = 0;
-    for (uint32_t t0 = 0; t0 < size; t0 += NT) {
-      const uint32_t i = t0 + tid;
-      const uint32_t id = i < size ? (qi[i] & kIdMask) : 0u;
-      const bool keep = i < size && id < P.n;
-      uint32_t total;
-      const uint32_t pos = base + block_scan<NT>(keep, M->warp_sums, total);
-      if (keep && pos < P.k) { out_ids[pos] = id; out_d[pos] = qd[i]; }
-      base += total;
-    }
-    written = min(base, P.k);
-  } else {
-    // Compact non-start candidates in queue order into cand_id, score them exactly.
-    uint32_t base = 0;
-    for (uint32_t t0 = 0; t0 < size; t0 += NT) {
-      const uint32_t i = t0 + tid;
-      const uint32_t id = i < size ? (qi[i] & kIdMask) : 0u;
-      const bool keep = i < size && id < P.n;
-      uint32_t total;
-      const uint32_t pos = base + block_scan<NT>(keep, M->warp_sums, total);
-      if (keep) S.cand_id[pos] = id;
-      base += total;
-    }
-    const uint32_t count = base;
-    __syncthreads();
-    score_candidates<NT, METRIC, false, DIM>(P, S, count);
-    __syncthreads();
-    // Stable rank by full-precision distance; NaN sorts last.
-    for (uint32_t i = tid; i < count; i += NT) {
-      const float d = S.cand_d[i];
-      const bool dn = d != d;
-      uint32_t r = 0;
-      for (uint32_t j = 0; j < count; ++j) {
-        const float dj = S.cand_d[j];
-        const bool jn = dj != dj;
-        const bool before = dn ? (jn && j < i) : (jn ? false : (dj < d || (dj == d && j < i)));
-        r += before;
-      }
-      if (r < P.k) { out_ids[r] = S.cand_id[i]; out_d[r] = d; }
-    }
-    written = min(count, P.k);
-  }
-  for (uint32_t j = written + tid; j < P.k; j += NT) {
-    out_ids[j] = DK_INVALID_ID;
-    out_d[j] = INFINITY;
-  }
-  if (tid == 0) M->pad = written;  // result_count, read by the caller after a barrier
-}
-
-// The whole search of one query.  Returns false if the visited set overflowed.
-template <int NT, int METRIC, bool PQ, int DIM, class VSet>
-__device__ bool search_one(const SearchParams& P, const State& S, const VSet& vset, uint32_t qid,
-                           uint32_t& cmps_out, uint32_t& hops_out) {
-  const uint32_t tid = threadIdx.x;
-  Misc* M = S.misc;
-  // Query into shared memory, zero padded to a multiple of 8 floats.
-  const float* qsrc = P.queries + (size_t)qid * P.qstride;
-  const uint32_t dpad = (P.dim + 7u) & ~7u;
-  for (uint32_t i = tid; i < dpad; i += NT) S.q[i] = i < P.dim ? qsrc[i] : 0.0f;
-  vset.clear(tid, NT);
-  if (tid == 0) {
-    M->size = 0;
-    M->cursor = 0;
-    M->cur = 0;
-    M->inserted = 0;
-    M->overflow = 0;
-  }
-  __syncthreads();
-  if (PQ) {
-    build_table<NT, METRIC>(P, S);
-    __syncthreads();
-  }
-  // A visited set too small for even the start points plus one hop goes to the spill pass.
-  if (P.f + P.beam * P.max_degree > P.hash_limit) return false;
-  // Start points (index.rs:1956-1963): visited, scored and inserted in order.
-  for (uint32_t s = tid; s < P.f; s += NT) {
-    S.cand_id[s] = P.n + s;
-    vset.insert(P.n + s);
-  }
-  if (tid == 0) M->inserted = P.f;
-  __syncthreads();
-  score_candidates<NT, METRIC, PQ, DIM>(P, S, P.f);
-  __syncthreads();
-  merge_batch<NT>(P, S, P.f);
-  uint32_t cmps = P.f, hops = 0;
-
-  while (true) {
-    // Pop up to beam_width closest unvisited nodes (queue.rs:297-313).
-    if (tid == 0) {
-      uint32_t nb = 0, c = M->cursor;
-      const uint32_t size = M->size;
-      uint32_t* qi = S.qi[M->cur];
-      while (nb < P.beam && c < size) {
-        const uint32_t id = qi[c] & kIdMask;
-        qi[c] |= kVisited;
-        M->beam[nb++] = id;
-        ++c;
-        while (c < size && (qi[c] & kVisited)) ++c;
-      }
-      M->cursor = c;
-      M->nbeam = nb;
-      if (nb && M->inserted + nb * P.max_degree > P.hash_limit) M->overflow = 1;
-    }
-    __syncthreads();
-    const uint32_t nb = M->nbeam;
-    if (nb == 0) break;
-    if (M->overflow) return false;
-    // Expand: adjacency rows in beam order, ids filtered through the visited set in order.
-    uint32_t count = 0;
-    for (uint32_t b = 0; b < nb; ++b) {
-      const uint32_t* row = P.adj + (size_t)M->beam[b] * P.astride;
-      const uint32_t deg = __ldg(row);
-      for (uint32_t t0 = 0; t0 < deg; t0 += NT) {
-        const uint32_t t = t0 + tid;
-        bool fresh = false;
-        uint32_t id = 0;
-        if (t < deg) {
-          id = __ldg(row + 1 + t);
-          fresh = vset.insert(id);
-        }
-        uint32_t total;
-        const uint32_t pos = block_scan<NT>(fresh, M->warp_sums, total);
-        if (fresh) S.cand_id[count + pos] = id;
-        count += total;
-      }
-    }
-    if (tid == 0) M->inserted += count;
-    __syncthreads();
-    score_candidates<NT, METRIC, PQ, DIM>(P, S, count);
-    __syncthreads();
-    merge_batch<NT>(P, S, count);
-    cmps += count;
-    hops += nb;
-  }
-  cmps_out = cmps;
-  hops_out = hops;
-  return true;
-}
-
-template <int NT, int METRIC, bool PQ, int DIM>
-__global__ void __launch_bounds__(NT) k_search_hash(const SearchParams P) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  const State S = carve(smem, P);
-  SmemHashSet vset;
-  vset.slots = reinterpret_cast<uint32_t*>(smem + P.off_hash);
-  vset.mask = (1u << P.hash_log2) - 1u;
-  vset.shift = 32u - P.hash_log2;
-  const uint32_t qid = blockIdx.x;
-  if (qid >= P.nq) return;
-  uint32_t cmps = 0, hops = 0;
-  const bool ok = search_one<NT, METRIC, PQ, DIM>(P, S, vset, qid, cmps, hops);
-  if (!ok) {
-    if (threadIdx.x == 0) {
-      dk_search_stats st = {0u, 0u, 0u, kFlagSpilled};
-      P.stats[qid] = st;
-    }
-    return;
-  }
-  post_process<NT, METRIC, DIM>(P, S, qid);
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    dk_search_stats st = {cmps, hops, S.misc->pad, 0u};
-    P.stats[qid] = st;
-    if (P.hint) atomicMax(P.hint, (uint32_t)(((uint64_t)cmps << 8) / P.cap));
-  }
-}
-
-// Spill pass: each CTA owns one bitmap slice and re-runs the queries the first pass flagged.
-template <int NT, int METRIC, bool PQ, int DIM>
-__global__ void __launch_bounds__(NT) k_search_spill(const SearchParams P) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  const State S = carve(smem, P);
-  BitmapSet vset;
-  vset.words = P.bitmap + (size_t)blockIdx.x * P.bitmap_words;
-  vset.nwords = P.bitmap_words;
-  for (uint32_t qid = blockIdx.x; qid < P.nq; qid += gridDim.x) {
-    if (!(P.stats[qid].flags & kFlagSpilled)) continue;
-    __syncthreads();
-    uint32_t cmps = 0, hops = 0;
-    search_one<NT, METRIC, PQ, DIM>(P, S, vset, qid, cmps, hops);
-    post_process<NT, METRIC, DIM>(P, S, qid);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      dk_search_stats st = {cmps, hops, S.misc->pad, kFlagSpilled};
-      P.stats[qid] = st;
-      if (P.hint) atomicMax(P.hint, (uint32_t)(((uint64_t)cmps << 8) / P.cap));
-    }
-    __syncthreads();
-  }
-}
-
-// ----------------------------------------------------------------------------------------
-// Host side: shared-memory plan and dispatch.
-// ----------------------------------------------------------------------------------------
-
-constexpr int kThreads = 128;
-
 inline uint32_t align_up(uint32_t x, uint32_t a) { return (x + a - 1) / a * a; }
 
-uint32_t plan_smem(SearchParams& P, bool pq, bool with_hash) {
+// Lay out one query's shared-memory state; returns its size in bytes.
+uint32_t plan_query_smem(SearchParams& P, bool pq, bool with_hash) {
   uint32_t off = 0;
   auto take = [&](uint32_t bytes) {
     const uint32_t o = off;
@@ -687,55 +34,9 @@ uint32_t plan_smem(SearchParams& P, bool pq, bool with_hash) {
   P.off_cand_d = take(P.list_cap * 4);
   P.off_new_d = take(P.list_cap * 4);
   P.off_new_id = take(P.list_cap * 4);
-  P.off_misc = take(sizeof(Misc));
+  P.off_misc = take(sizeof(dk::Misc));
   P.off_hash = take(with_hash ? (4u << P.hash_log2) : 0u);
-  P.smem_bytes = off;
   return off;
-}
-
-template <int METRIC, bool PQ, int DIM>
-cudaError_t launch_variant(const SearchParams& P1, const SearchParams& P2, uint32_t spill_ctas,
-                           cudaStream_t stream) {
-  auto k1 = k_search_hash<kThreads, METRIC, PQ, DIM>;
-  auto k2 = k_search_spill<kThreads, METRIC, PQ, DIM>;
-  cudaError_t e = cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)P1.smem_bytes);
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P2.smem_bytes);
-  if (e != cudaSuccess) return e;
-  k1<<<P1.nq, kThreads, P1.smem_bytes, stream>>>(P1);
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  k2<<<spill_ctas, kThreads, P2.smem_bytes, stream>>>(P2);
-  return cudaGetLastError();
-}
-
-template <int METRIC, bool PQ>
-cudaError_t launch_metric(const SearchParams& P1, const SearchParams& P2, uint32_t spill_ctas,
-                          cudaStream_t stream) {
-  switch (P1.dim) {
-    case 96: return launch_variant<METRIC, PQ, 96>(P1, P2, spill_ctas, stream);
-    case 128: return launch_variant<METRIC, PQ, 128>(P1, P2, spill_ctas, stream);
-    case 384: return launch_variant<METRIC, PQ, 384>(P1, P2, spill_ctas, stream);
-    case 768: return launch_variant<METRIC, PQ, 768>(P1, P2, spill_ctas, stream);
-    default: return launch_variant<METRIC, PQ, 0>(P1, P2, spill_ctas, stream);
-  }
-}
-
-template <bool PQ>
-cudaError_t launch_pq(int32_t metric, const SearchParams& P1, const SearchParams& P2,
-                      uint32_t spill_ctas, cudaStream_t stream) {
-  switch (metric) {
-    case DK_METRIC_L2: return launch_metric<DK_METRIC_L2, PQ>(P1, P2, spill_ctas, stream);
-    case DK_METRIC_INNER_PRODUCT:
-      return launch_metric<DK_METRIC_INNER_PRODUCT, PQ>(P1, P2, spill_ctas, stream);
-    case DK_METRIC_COSINE_NORMALIZED:
-      return launch_metric<DK_METRIC_COSINE_NORMALIZED, PQ>(P1, P2, spill_ctas, stream);
-    default:
-      // PQ traversal with Cosine uses direct reconstruction in the reference
-      // (pq/distance/cosine.rs); it is rejected by the API before reaching here.
-      return launch_metric<DK_METRIC_COSINE, false>(P1, P2, spill_ctas, stream);
-  }
 }
 
 uint32_t env_u32(const char* name, uint32_t dflt) {
@@ -757,6 +58,7 @@ int32_t dk_launch_search(const dk_index* ix, int32_t strategy, const float* quer
   P.adj = ix->adj;
   P.codes = ix->codes;
   P.pivots = ix->pivots;
+  P.pivots_cm = ix->pivots_cm;
   P.offsets = ix->offsets;
   P.n = ix->n;
   P.f = ix->f;
@@ -800,26 +102,51 @@ int32_t dk_launch_search(const dk_index* ix, int32_t strategy, const float* quer
   uint32_t log2h = 9;
   while ((double)(1u << log2h) * 0.75 < est && log2h < 16) ++log2h;
   log2h = env_u32("DK_HASH_LOG2", log2h);
-  if (log2h < 6) log2h = 6;
-  if (log2h > 20) log2h = 20;
-  P.hash_log2 = log2h;
-  P.hash_limit = (uint32_t)((1u << log2h) * 0.75);
-
-  SearchParams P2 = P;
-  P2.hash_limit = 0xFFFFFFFFu;  // the bitmap never fills
-  plan_smem(P, pq, true);
-  plan_smem(P2, pq, false);
+  log2h = std::min<uint32_t>(std::max<uint32_t>(log2h, 6), 20);
 
   int dev = 0, max_optin = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  while (P.smem_bytes > (uint32_t)max_optin && P.hash_log2 > 6) {
-    --P.hash_log2;
+
+  dk::LaunchPlan L{};
+  // Kernel choice: one warp per query unless rows are wide (D >= 384) or the beam is wide,
+  // where a 128-thread CTA scores more candidates per round.  DK_KERNEL=warp|cta overrides.
+  const char* kenv = getenv("DK_KERNEL");
+  bool warp = ix->dim < 384 && beam <= 4;
+  if (kenv && !strcmp(kenv, "warp")) warp = true;
+  if (kenv && !strcmp(kenv, "cta")) warp = false;
+
+  P.hash_log2 = log2h;
+  while (true) {
     P.hash_limit = (uint32_t)((1u << P.hash_log2) * 0.75);
-    plan_smem(P, pq, true);
+    const uint32_t bytes = plan_query_smem(P, pq, true);
+    if (warp) {
+      P.warp_smem = bytes;
+      uint32_t wpc = std::min<uint32_t>(4, (uint32_t)max_optin / std::max<uint32_t>(bytes, 1));
+      if (wpc >= 1) {
+        L.kind = dk::KernelKind::kWarp;
+        L.warps_per_cta = wpc;
+        P.smem_bytes = bytes * wpc;
+        break;
+      }
+    } else if (bytes <= (uint32_t)max_optin) {
+      L.kind = dk::KernelKind::kCta;
+      P.smem_bytes = bytes;
+      break;
+    }
+    if (P.hash_log2 <= 6) {
+      dk_set_error(DK_ERR_UNSUPPORTED, "search state does not fit in shared memory (L or PQ too large)");
+      return DK_ERR_UNSUPPORTED;
+    }
+    --P.hash_log2;
   }
-  if (P.smem_bytes > (uint32_t)max_optin || P2.smem_bytes > (uint32_t)max_optin) {
+  L.p1 = P;
+
+  SearchParams P2 = P;
+  P2.hash_limit = 0xFFFFFFFFu;  // the bitmap never fills
+  P2.smem_bytes = plan_query_smem(P2, pq, false);
+  if (P2.smem_bytes > (uint32_t)max_optin) {
     dk_set_error(DK_ERR_UNSUPPORTED, "search state does not fit in shared memory (L or PQ too large)");
     return DK_ERR_UNSUPPORTED;
   }
@@ -838,9 +165,15 @@ int32_t dk_launch_search(const dk_index* ix, int32_t strategy, const float* quer
   }
   P2.bitmap = bitmap;
   P2.bitmap_words = words;
+  L.p2 = P2;
+  L.spill_ctas = spill_ctas;
 
-  if (pq) e = launch_pq<true>(ix->metric, P, P2, spill_ctas, stream);
-  else e = launch_pq<false>(ix->metric, P, P2, spill_ctas, stream);
+  switch (ix->metric) {
+    case DK_METRIC_L2: e = dk_launch_l2(L, pq, stream); break;
+    case DK_METRIC_INNER_PRODUCT: e = dk_launch_ip(L, pq, stream); break;
+    case DK_METRIC_COSINE: e = dk_launch_cosine(L, pq, stream); break;
+    default: e = dk_launch_cosine_normalized(L, pq, stream); break;
+  }
   cudaFreeAsync(bitmap, stream);
   if (e != cudaSuccess) {
     dk_set_error(DK_ERR_CUDA, std::string("search launch: ") + cudaGetErrorString(e));
