@@ -56,6 +56,12 @@ struct SearchParams {
   uint32_t hash_limit;  // inserts allowed before the hash counts as full
   uint32_t* bitmap;
   uint32_t bitmap_words;
+  // Warp kernel: persistent work counter and each warp's global overflow hash (second level
+  // of the visited set, used once the shared hash holds `hash_limit` ids).
+  uint32_t* work_counter;
+  uint32_t* gtable;
+  uint32_t gtable_log2;
+  uint32_t gtable_limit;
   // Shared-memory carve-up: byte offsets from the CTA's dynamic shared memory (CTA kernel)
   // or from the warp's slice of it (warp kernel, slices of `warp_smem` bytes).
   uint32_t off_query, off_table, off_qd0, off_qi0, off_qd1, off_qi1;

@@ -96,6 +96,61 @@ struct BitmapSet {
   }
 };
 
+// Exact visited set in two levels: a small shared-memory hash takes the first `slimit` ids;
+// once it holds that many it stops accepting, and every later new id goes to a larger
+// open-addressing hash in global memory (one per warp).  The shared level never changes
+// after it fills, so "absent from the shared level" followed by a global probe is exact.
+// Ids reaching `insert` in one round are distinct (adjacency lists are de-duplicated when
+// the index is built and beam rows are filtered one after another).
+struct TwoLevelSet {
+  uint32_t* s;
+  uint32_t smask, sshift, slimit;
+  uint32_t* scount;  // shared: ids accepted by the shared level (may overshoot slimit)
+  uint32_t* g;
+  uint32_t gmask, gshift;
+  uint32_t* gcount;  // shared: ids stored in the global level
+
+  __device__ void reset(uint32_t lane) const {
+    for (uint32_t i = lane; i <= smask; i += 32u) s[i] = kEmpty;
+    if (lane == 0) {
+      *scount = 0u;
+      *gcount = 0u;
+    }
+  }
+  __device__ bool insert(uint32_t id) const {
+    volatile uint32_t* vs = s;
+    uint32_t h = (id * 2654435761u) >> sshift;
+    while (true) {
+      const uint32_t cur = vs[h];
+      if (cur == id) return false;
+      if (cur == kEmpty) break;
+      h = (h + 1) & smask;
+    }
+    if (*(volatile uint32_t*)scount < slimit && atomicAdd(scount, 1u) < slimit) {
+      // A slot of the shared level is reserved for this id: take the next empty one.
+      while (atomicCAS(&s[h], kEmpty, id) != kEmpty) {
+        do { h = (h + 1) & smask; } while (vs[h] != kEmpty);
+      }
+      return true;
+    }
+    volatile uint32_t* vg = g;
+    uint32_t hg = ((id ^ 0x5bd1e995u) * 0x9E3779B1u) >> gshift;
+    while (true) {
+      const uint32_t cur = vg[hg];
+      if (cur == id) return false;
+      if (cur == kEmpty) {
+        const uint32_t old = atomicCAS(&g[hg], kEmpty, id);
+        if (old == kEmpty) {
+          atomicAdd(gcount, 1u);
+          return true;
+        }
+        if (old == id) return false;
+      }
+      hg = (hg + 1) & gmask;
+    }
+  }
+};
+
 // ----------------------------------------------------------------------------------------
 // Small helpers.
 // ----------------------------------------------------------------------------------------
@@ -430,6 +485,7 @@ __device__ __forceinline__ void build_table(const SearchParams& P, const float* 
 
 struct Misc {
   uint32_t size, cursor, cur, nbeam, nvalid, inserted, overflow, result_count;
+  uint32_t scount, gcount, pad0, pad1;  // warp kernel: two-level visited-set counters
   uint32_t beam[64];
   uint32_t warp_sums[32];
 };
@@ -824,29 +880,24 @@ __device__ void warp_post_process(const SearchParams& P, const State& S, uint32_
   result_count = written;
 }
 
+// One query, run by one warp.  Writes the query's outputs and stats (or the spill flag).
 template <int METRIC, bool PQ, int DIM, int U>
-__global__ void __launch_bounds__(128) k_search_warp(const SearchParams P) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-  const uint32_t qid = blockIdx.x * (blockDim.x >> 5) + warp;
-  if (qid >= P.nq) return;  // whole warp; no block-level synchronisation below
-  const State S = carve(smem + (size_t)warp * P.warp_smem, P);
-  const SmemHashSet vset{S.hash, (1u << P.hash_log2) - 1u, 32u - P.hash_log2};
-
+__device__ __forceinline__ void warp_query(const SearchParams& P, const State& S,
+                                           const TwoLevelSet& vset, uint32_t qid, uint32_t lane) {
   const float* qsrc = P.queries + (size_t)qid * P.qstride;
   const uint32_t dpad = (P.dim + 7u) & ~7u;
   for (uint32_t i = lane; i < dpad; i += 32u) S.q[i] = i < P.dim ? qsrc[i] : 0.0f;
-  vset.clear(lane, 32u);
+  vset.reset(lane);
   __syncwarp();
   if (PQ) {
     build_table<METRIC>(P, S.q, S.table, lane, 32u);
     __syncwarp();
   }
-  if (P.f + P.beam * P.max_degree > P.hash_limit) {
+  if (P.f + P.beam * P.max_degree > P.gtable_limit) {
     if (lane == 0) P.stats[qid] = dk_search_stats{0u, 0u, 0u, kFlagSpilled};
     return;
   }
-  uint32_t size = 0, cursor = 0, cur = 0, inserted = P.f;
+  uint32_t size = 0, cursor = 0, cur = 0;
   for (uint32_t s = lane; s < P.f; s += 32u) {
     S.cand_id[s] = P.n + s;
     vset.insert(P.n + s);
@@ -883,7 +934,8 @@ __global__ void __launch_bounds__(128) k_search_warp(const SearchParams P) {
     }
     cursor = min(c, size);
     __syncwarp();
-    if (inserted + nb * P.max_degree > P.hash_limit) {
+    // The global level must keep room for a whole hop going there; otherwise spill.
+    if (*(volatile uint32_t*)vset.gcount + nb * P.max_degree > P.gtable_limit) {
       if (lane == 0) P.stats[qid] = dk_search_stats{0u, 0u, 0u, kFlagSpilled};
       return;
     }
@@ -913,7 +965,6 @@ __global__ void __launch_bounds__(128) k_search_warp(const SearchParams P) {
         count += __popc(m);
       }
     }
-    inserted += count;
     __syncwarp();
     warp_score<METRIC, PQ, DIM, U>(P, S, S.cand_id, S.cand_d, count, lane);
     warp_merge(P, S, count, lane, size, cursor, cur);
@@ -928,6 +979,40 @@ __global__ void __launch_bounds__(128) k_search_warp(const SearchParams P) {
   }
 }
 
+// Persistent grid: every warp owns a shared-memory slice and a global overflow table and
+// takes queries from a work counter until the batch is done.
+template <int METRIC, bool PQ, int DIM, int U>
+__global__ void __launch_bounds__(128) k_search_warp(const SearchParams P) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  const uint32_t slot = blockIdx.x * (blockDim.x >> 5) + warp;
+  const State S = carve(smem + (size_t)warp * P.warp_smem, P);
+  TwoLevelSet vset;
+  vset.s = S.hash;
+  vset.smask = (1u << P.hash_log2) - 1u;
+  vset.sshift = 32u - P.hash_log2;
+  vset.slimit = P.hash_limit;
+  vset.scount = &S.misc->scount;
+  vset.g = P.gtable + ((size_t)slot << P.gtable_log2);
+  vset.gmask = (1u << P.gtable_log2) - 1u;
+  vset.gshift = 32u - P.gtable_log2;
+  vset.gcount = &S.misc->gcount;
+  bool gdirty = true;  // the overflow table starts as uninitialised memory
+  while (true) {
+    uint32_t qid = 0;
+    if (lane == 0) qid = atomicAdd(P.work_counter, 1u);
+    qid = __shfl_sync(kFull, qid, 0);
+    if (qid >= P.nq) break;
+    if (gdirty) {
+      for (uint32_t i = lane; i <= vset.gmask; i += 32u) vset.g[i] = kEmpty;
+      __syncwarp();
+    }
+    warp_query<METRIC, PQ, DIM, U>(P, S, vset, qid, lane);
+    __syncwarp();
+    gdirty = *(volatile uint32_t*)vset.gcount != 0u;
+  }
+}
+
 // ========================================================================================
 // Launch helpers (host).
 // ========================================================================================
@@ -939,12 +1024,14 @@ struct LaunchPlan {
   SearchParams p2;     // spill pass (CTA layout, bitmap)
   KernelKind kind;
   uint32_t warps_per_cta;
+  uint32_t grid;       // warp kernel: persistent grid size
   uint32_t spill_ctas;
-  uint32_t launches;   // kernels launched (reported to callers that count them)
+  bool query_only;     // warp kernel: only report `blocks_per_sm` for `warps_per_cta`
+  int blocks_per_sm;
 };
 
 template <int METRIC, bool PQ, int DIM>
-cudaError_t launch_variant(const LaunchPlan& L, cudaStream_t stream) {
+cudaError_t launch_variant(LaunchPlan& L, cudaStream_t stream) {
   cudaError_t e;
   constexpr int U = (DIM > 0 && DIM <= 128) ? 2 : 1;
   if (L.kind == KernelKind::kWarp) {
@@ -952,8 +1039,11 @@ cudaError_t launch_variant(const LaunchPlan& L, cudaStream_t stream) {
     const uint32_t bytes = L.p1.warp_smem * L.warps_per_cta;
     e = cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (e != cudaSuccess) return e;
-    const uint32_t grid = (L.p1.nq + L.warps_per_cta - 1) / L.warps_per_cta;
-    k1<<<grid, 32 * L.warps_per_cta, bytes, stream>>>(L.p1);
+    if (L.query_only) {
+      return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&L.blocks_per_sm, k1,
+                                                           32 * L.warps_per_cta, bytes);
+    }
+    k1<<<L.grid, 32 * L.warps_per_cta, bytes, stream>>>(L.p1);
   } else {
     auto k1 = k_search_cta<kCtaThreads, METRIC, PQ, DIM>;
     e = cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.p1.smem_bytes);
@@ -970,7 +1060,7 @@ cudaError_t launch_variant(const LaunchPlan& L, cudaStream_t stream) {
 }
 
 template <int METRIC, bool PQ>
-cudaError_t launch_dims(const LaunchPlan& L, cudaStream_t stream) {
+cudaError_t launch_dims(LaunchPlan& L, cudaStream_t stream) {
   switch (L.p1.dim) {
     case 96: return launch_variant<METRIC, PQ, 96>(L, stream);
     case 128: return launch_variant<METRIC, PQ, 128>(L, stream);
@@ -983,7 +1073,7 @@ cudaError_t launch_dims(const LaunchPlan& L, cudaStream_t stream) {
 }  // namespace dk
 
 // Per-metric entry points (one translation unit each, compiled in parallel).
-cudaError_t dk_launch_l2(const dk::LaunchPlan& L, bool pq, cudaStream_t stream);
-cudaError_t dk_launch_ip(const dk::LaunchPlan& L, bool pq, cudaStream_t stream);
-cudaError_t dk_launch_cosine(const dk::LaunchPlan& L, bool pq, cudaStream_t stream);
-cudaError_t dk_launch_cosine_normalized(const dk::LaunchPlan& L, bool pq, cudaStream_t stream);
+cudaError_t dk_launch_l2(dk::LaunchPlan& L, bool pq, cudaStream_t stream);
+cudaError_t dk_launch_ip(dk::LaunchPlan& L, bool pq, cudaStream_t stream);
+cudaError_t dk_launch_cosine(dk::LaunchPlan& L, bool pq, cudaStream_t stream);
+cudaError_t dk_launch_cosine_normalized(dk::LaunchPlan& L, bool pq, cudaStream_t stream);

@@ -1,5 +1,5 @@
-// Host side of the batched search: shared-memory planning, visited-set sizing, kernel choice
-// and the two-pass launch (first pass with a shared-memory hash, spill pass with a bitmap).
+// Host side of the batched search: shared-memory planning, visited-set sizing, kernel choice,
+// occupancy and scratch, then the first pass (warp or CTA kernel) and the spill pass.
 // Device code is in dk_kernels.cuh; per-metric instantiations in dk_search_<metric>.cu.
 
 #include <cuda_runtime.h>
@@ -15,6 +15,7 @@
 namespace {
 
 inline uint32_t align_up(uint32_t x, uint32_t a) { return (x + a - 1) / a * a; }
+inline uint64_t align_up64(uint64_t x, uint64_t a) { return (x + a - 1) / a * a; }
 
 // Lay out one query's shared-memory state; returns its size in bytes.
 uint32_t plan_query_smem(SearchParams& P, bool pq, bool with_hash) {
@@ -43,6 +44,26 @@ uint32_t env_u32(const char* name, uint32_t dflt) {
   const char* v = getenv(name);
   if (!v || !*v) return dflt;
   return (uint32_t)strtoul(v, nullptr, 10);
+}
+
+uint32_t log2_at_least(double x, uint32_t lo, uint32_t hi) {
+  uint32_t l = lo;
+  while (l < hi && (double)(1u << l) < x) ++l;
+  return l;
+}
+
+cudaError_t dispatch(int32_t metric, dk::LaunchPlan& L, bool pq, cudaStream_t stream) {
+  switch (metric) {
+    case DK_METRIC_L2: return dk_launch_l2(L, pq, stream);
+    case DK_METRIC_INNER_PRODUCT: return dk_launch_ip(L, pq, stream);
+    case DK_METRIC_COSINE: return dk_launch_cosine(L, pq, stream);
+    default: return dk_launch_cosine_normalized(L, pq, stream);
+  }
+}
+
+int32_t too_big() {
+  dk_set_error(DK_ERR_UNSUPPORTED, "search state does not fit in shared memory (L or PQ too large)");
+  return DK_ERR_UNSUPPORTED;
 }
 
 }  // namespace
@@ -81,12 +102,12 @@ int32_t dk_launch_search(const dk_index* ix, int32_t strategy, const float* quer
   P.stats = stats;
   P.list_cap = std::max(std::max(beam * ix->max_degree, P.cap), ix->f);
 
-  // Visited-set hash.  |visited| equals the comparison count, which for a given graph grows
-  // about linearly with L + F.  The ratio is learned from previous launches on this index
-  // (kernels record their largest cmps / (L + F) in mapped host memory); before any launch
-  // the prior is half the reference's own upper-bound estimate (scratch.rs:186-193,
-  // 1.1 * max_degree * 1.3 * L).  The hash is sized to stay under 3/4 load for the learned
-  // ratio plus one hop; a query that needs more re-runs exactly in the bitmap spill pass.
+  // Visited-set size.  |visited| equals the comparison count, which for a given graph grows
+  // about linearly with L + F.  The largest ratio is learned from previous launches on this
+  // index (kernels record cmps / (L + F) in mapped host memory); before any launch the
+  // prior is half the reference's own upper-bound estimate (scratch.rs:186-193,
+  // 1.1 * max_degree * 1.3 * L).  Only performance depends on these sizes: a query whose
+  // visited set outgrows them re-runs exactly in the bitmap spill pass.
   double ratio = 0.5 * 1.1 * 1.3 * ix->max_degree;
   P.hint = ix->hint_dev;
   if (ix->hint_host) {
@@ -99,17 +120,12 @@ int32_t dk_launch_search(const dk_index* ix, int32_t strategy, const float* quer
     if (h[1]) ratio = (double)h[1] / 256.0 * 1.15;
   }
   const double est = ratio * (double)P.cap + beam * ix->max_degree + ix->f;
-  uint32_t log2h = 9;
-  while ((double)(1u << log2h) * 0.75 < est && log2h < 16) ++log2h;
-  log2h = env_u32("DK_HASH_LOG2", log2h);
-  log2h = std::min<uint32_t>(std::max<uint32_t>(log2h, 6), 20);
 
   int dev = 0, max_optin = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
 
-  dk::LaunchPlan L{};
   // Kernel choice: one warp per query unless rows are wide (D >= 384) or the beam is wide,
   // where a 128-thread CTA scores more candidates per round.  DK_KERNEL=warp|cta overrides.
   const char* kenv = getenv("DK_KERNEL");
@@ -117,64 +133,93 @@ int32_t dk_launch_search(const dk_index* ix, int32_t strategy, const float* quer
   if (kenv && !strcmp(kenv, "warp")) warp = true;
   if (kenv && !strcmp(kenv, "cta")) warp = false;
 
-  P.hash_log2 = log2h;
-  while (true) {
+  dk::LaunchPlan L{};
+  uint64_t gtable_bytes = 0;
+  cudaError_t e = cudaSuccess;
+  if (warp) {
+    // Small shared level sized to a per-warp shared-memory budget (many queries per SM);
+    // the global level holds the rest of the learned visited-set size.
+    L.kind = dk::KernelKind::kWarp;
+    P.hash_log2 = 0;
+    const uint32_t base = plan_query_smem(P, pq, false);
+    const uint32_t budget = std::max<uint32_t>(env_u32("DK_WARP_SMEM", 8192), base + 1024);
+    uint32_t hl = 8;
+    while (hl < 16 && base + (4u << (hl + 1)) <= budget) ++hl;
+    P.hash_log2 = env_u32("DK_HASH_LOG2", hl);
+    P.hash_log2 = std::min<uint32_t>(std::max<uint32_t>(P.hash_log2, 6), 16);
     P.hash_limit = (uint32_t)((1u << P.hash_log2) * 0.75);
-    const uint32_t bytes = plan_query_smem(P, pq, true);
-    if (warp) {
-      P.warp_smem = bytes;
-      uint32_t wpc = std::min<uint32_t>(4, (uint32_t)max_optin / std::max<uint32_t>(bytes, 1));
-      if (wpc >= 1) {
-        L.kind = dk::KernelKind::kWarp;
-        L.warps_per_cta = wpc;
-        P.smem_bytes = bytes * wpc;
-        break;
+    P.warp_smem = plan_query_smem(P, pq, true);
+    if (P.warp_smem > (uint32_t)max_optin) return too_big();
+    P.gtable_log2 = log2_at_least(std::max(est, 2.0 * P.hash_limit) / 0.75, 10, 22);
+    P.gtable_limit = (uint32_t)((1u << P.gtable_log2) * 0.75);
+    // Warps per CTA: the packing with the most resident warps per SM.
+    int best_warps = 0;
+    for (uint32_t wpc : {4u, 2u, 1u}) {
+      if (P.warp_smem * wpc > (uint32_t)max_optin) continue;
+      dk::LaunchPlan Q{};
+      Q.kind = dk::KernelKind::kWarp;
+      Q.p1 = P;
+      Q.warps_per_cta = wpc;
+      Q.query_only = true;
+      e = dispatch(ix->metric, Q, pq, stream);
+      if (e != cudaSuccess) {
+        dk_set_error(DK_ERR_CUDA, std::string("occupancy query: ") + cudaGetErrorString(e));
+        return DK_ERR_CUDA;
       }
-    } else if (bytes <= (uint32_t)max_optin) {
-      L.kind = dk::KernelKind::kCta;
-      P.smem_bytes = bytes;
-      break;
+      if (Q.blocks_per_sm * (int)wpc > best_warps) {
+        best_warps = Q.blocks_per_sm * (int)wpc;
+        L.warps_per_cta = wpc;
+        L.blocks_per_sm = Q.blocks_per_sm;
+      }
     }
-    if (P.hash_log2 <= 6) {
-      dk_set_error(DK_ERR_UNSUPPORTED, "search state does not fit in shared memory (L or PQ too large)");
-      return DK_ERR_UNSUPPORTED;
+    if (best_warps == 0) return too_big();
+    const uint32_t want = (nq + L.warps_per_cta - 1) / L.warps_per_cta;
+    L.grid = std::min<uint32_t>(want, (uint32_t)L.blocks_per_sm * (uint32_t)sms);
+    gtable_bytes = (uint64_t)L.grid * L.warps_per_cta * (4ull << P.gtable_log2);
+  } else {
+    L.kind = dk::KernelKind::kCta;
+    uint32_t log2h = log2_at_least(est / 0.75, 9, 16);
+    log2h = env_u32("DK_HASH_LOG2", log2h);
+    P.hash_log2 = std::min<uint32_t>(std::max<uint32_t>(log2h, 6), 20);
+    while (true) {
+      P.hash_limit = (uint32_t)((1u << P.hash_log2) * 0.75);
+      P.smem_bytes = plan_query_smem(P, pq, true);
+      if (P.smem_bytes <= (uint32_t)max_optin) break;
+      if (P.hash_log2 <= 6) return too_big();
+      --P.hash_log2;
     }
-    --P.hash_log2;
   }
-  L.p1 = P;
 
   SearchParams P2 = P;
   P2.hash_limit = 0xFFFFFFFFu;  // the bitmap never fills
   P2.smem_bytes = plan_query_smem(P2, pq, false);
-  if (P2.smem_bytes > (uint32_t)max_optin) {
-    dk_set_error(DK_ERR_UNSUPPORTED, "search state does not fit in shared memory (L or PQ too large)");
-    return DK_ERR_UNSUPPORTED;
-  }
+  if (P2.smem_bytes > (uint32_t)max_optin) return too_big();
 
-  // Spill pass scratch: one bitmap over all ids per spill CTA.
+  // Scratch, one stream-ordered allocation: work counter | global tables | spill bitmaps.
   const uint32_t words = (ix->n + ix->f + 31u) / 32u;
   uint32_t spill_ctas = std::min<uint32_t>(nq, (uint32_t)std::max(1, sms));
   const uint64_t per = (uint64_t)words * 4u;
   const uint64_t budget = 256ull << 20;
   if (per * spill_ctas > budget) spill_ctas = (uint32_t)std::max<uint64_t>(1, budget / per);
-  uint32_t* bitmap = nullptr;
-  cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&bitmap), per * spill_ctas, stream);
+  const uint64_t off_gtable = 256;
+  const uint64_t off_bitmap = align_up64(off_gtable + gtable_bytes, 256);
+  const uint64_t total = off_bitmap + per * spill_ctas;
+  unsigned char* scratch = nullptr;
+  e = cudaMallocAsync(reinterpret_cast<void**>(&scratch), total, stream);
   if (e != cudaSuccess) {
     dk_set_error(DK_ERR_OUT_OF_MEMORY, std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
     return DK_ERR_OUT_OF_MEMORY;
   }
-  P2.bitmap = bitmap;
+  e = cudaMemsetAsync(scratch, 0, 256, stream);
+  P.work_counter = reinterpret_cast<uint32_t*>(scratch);
+  P.gtable = reinterpret_cast<uint32_t*>(scratch + off_gtable);
+  P2.bitmap = reinterpret_cast<uint32_t*>(scratch + off_bitmap);
   P2.bitmap_words = words;
+  L.p1 = P;
   L.p2 = P2;
   L.spill_ctas = spill_ctas;
-
-  switch (ix->metric) {
-    case DK_METRIC_L2: e = dk_launch_l2(L, pq, stream); break;
-    case DK_METRIC_INNER_PRODUCT: e = dk_launch_ip(L, pq, stream); break;
-    case DK_METRIC_COSINE: e = dk_launch_cosine(L, pq, stream); break;
-    default: e = dk_launch_cosine_normalized(L, pq, stream); break;
-  }
-  cudaFreeAsync(bitmap, stream);
+  if (e == cudaSuccess) e = dispatch(ix->metric, L, pq, stream);
+  cudaFreeAsync(scratch, stream);
   if (e != cudaSuccess) {
     dk_set_error(DK_ERR_CUDA, std::string("search launch: ") + cudaGetErrorString(e));
     return DK_ERR_CUDA;

@@ -54,11 +54,18 @@ def test_grid_golden_through_abi(case):
     assert int(st[0]["result_count"]) == case["num_results"]
 
 
+@pytest.fixture(params=["warp", "cta"])
+def kernel(request, monkeypatch):
+    """Run a test with the warp-per-query kernel and with the CTA-per-query kernel."""
+    monkeypatch.setenv("DK_KERNEL", request.param)
+    return request.param
+
+
 @pytest.mark.parametrize("metric", [Metric.L2, Metric.INNER_PRODUCT, Metric.COSINE,
                                     Metric.COSINE_NORMALIZED])
 @pytest.mark.parametrize("dim", [3, 100, 128])
 @pytest.mark.parametrize("beam", [1, 4])
-def test_full_precision_parity(metric, dim, beam):
+def test_full_precision_parity(metric, dim, beam, kernel):
     norm = metric in (Metric.COSINE_NORMALIZED, Metric.INNER_PRODUCT)
     v, a, d, n = random_index(3000, dim, 24, seed=dim + beam, normalize=norm, max_degree=31)
     q = queries_like(v[:n], 64, seed=11, normalize=norm)
@@ -70,7 +77,7 @@ def test_full_precision_parity(metric, dim, beam):
 
 
 @pytest.mark.parametrize("dim", [96, 384, 768])
-def test_full_precision_parity_benchmark_dims(dim):
+def test_full_precision_parity_benchmark_dims(dim, kernel):
     v, a, d, n = random_index(2000, dim, 20, seed=dim, max_degree=26)
     q = queries_like(v[:n], 32, seed=5)
     idx = DiskANNIndex(GpuProvider(v, a, d, n, Metric.L2))
@@ -81,7 +88,7 @@ def test_full_precision_parity_benchmark_dims(dim):
 
 @pytest.mark.parametrize("metric", [Metric.L2, Metric.INNER_PRODUCT, Metric.COSINE_NORMALIZED])
 @pytest.mark.parametrize("strategy", ["hybrid", "quantized"])
-def test_pq_parity(metric, strategy):
+def test_pq_parity(metric, strategy, kernel):
     norm = metric != Metric.L2
     v, a, d, n = random_index(3000, 64, 24, seed=21, normalize=norm, max_degree=31)
     off, piv, codes = simple_pq(v, 16, seed=22)
@@ -93,7 +100,7 @@ def test_pq_parity(metric, strategy):
         assert_same(idx.search(Knn(k, l, bw), s, q), orc.search(q, k, l, bw, os_, threads=4))
 
 
-def test_spill_pass_is_exact(monkeypatch):
+def test_spill_pass_is_exact(monkeypatch, kernel):
     """A visited set forced past its shared-memory hash runs in the bitmap pass, same results."""
     v, a, d, n = random_index(4000, 32, 30, seed=31, max_degree=30)
     q = queries_like(v[:n], 40, seed=32)
@@ -109,7 +116,7 @@ def test_spill_pass_is_exact(monkeypatch):
     assert_same(gpu2, ref)
 
 
-def test_multiple_frozen_points_and_duplicates():
+def test_multiple_frozen_points_and_duplicates(kernel):
     """Two start points; adjacency lists with repeated ids (the visited set drops repeats)."""
     v, a, d, n = random_index(1500, 16, 12, seed=41, frozen=2, max_degree=16)
     rng = np.random.default_rng(42)
@@ -124,7 +131,7 @@ def test_multiple_frozen_points_and_duplicates():
                 orc.search(q, 10, 40, 2, O.STRATEGY_FULL_PRECISION))
 
 
-def test_nan_vectors_are_scored_not_inserted():
+def test_nan_vectors_are_scored_not_inserted(kernel):
     v, a, d, n = random_index(800, 8, 10, seed=51, max_degree=10)
     v[::7, 3] = np.nan
     q = queries_like(np.nan_to_num(v[:n]), 16, seed=52)
@@ -134,7 +141,7 @@ def test_nan_vectors_are_scored_not_inserted():
                 orc.search(q, 10, 30, 1, O.STRATEGY_FULL_PRECISION))
 
 
-def test_k_equals_l_and_small_graph():
+def test_k_equals_l_and_small_graph(kernel):
     v, a, d, n = random_index(50, 4, 6, seed=61, max_degree=6)
     q = queries_like(v[:n], 8, seed=62)
     idx = DiskANNIndex(GpuProvider(v, a, d, n, Metric.L2))
