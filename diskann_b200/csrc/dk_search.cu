@@ -151,6 +151,7 @@ int32_t dk_launch_search(const dk_index* ix, int32_t strategy, const float* quer
     P.warp_smem = plan_query_smem(P, pq, true);
     if (P.warp_smem > (uint32_t)max_optin) return too_big();
     P.gtable_log2 = log2_at_least(std::max(est, 2.0 * P.hash_limit) / 0.75, 10, 22);
+    P.gtable_log2 = std::min<uint32_t>(std::max<uint32_t>(env_u32("DK_GTABLE_LOG2", P.gtable_log2), 6), 24);
     P.gtable_limit = (uint32_t)((1u << P.gtable_log2) * 0.75);
     // Warps per CTA: the packing with the most resident warps per SM.
     int best_warps = 0;

@@ -101,17 +101,27 @@ def test_pq_parity(metric, strategy, kernel):
 
 
 def test_spill_pass_is_exact(monkeypatch, kernel):
-    """A visited set forced past its shared-memory hash runs in the bitmap pass, same results."""
+    """A visited set forced past its first-pass capacity runs in the bitmap spill pass with
+    the same results; the warp kernel's global second level is exact as well."""
     v, a, d, n = random_index(4000, 32, 30, seed=31, max_degree=30)
     q = queries_like(v[:n], 40, seed=32)
     idx = DiskANNIndex(GpuProvider(v, a, d, n, Metric.L2))
     orc = O.OracleIndex(v, a, d, n, O.METRIC_L2)
     ref = orc.search(q, 10, 200, 1, O.STRATEGY_FULL_PRECISION, threads=4)
+    # Tiny shared level: the warp kernel's visited set lives mostly in the global level.
+    monkeypatch.setenv("DK_HASH_LOG2", "6")
+    gpu = idx.search(Knn(10, 200), FullPrecision(), q)
+    assert_same(gpu, ref)
+    if kernel == "cta":
+        assert (gpu[2]["flags"] & 1).all()
+    # Both levels too small: every query spills.
     monkeypatch.setenv("DK_HASH_LOG2", "8")
+    monkeypatch.setenv("DK_GTABLE_LOG2", "8")
     gpu = idx.search(Knn(10, 200), FullPrecision(), q)
     assert (gpu[2]["flags"] & 1).any()
     assert_same(gpu, ref)
     monkeypatch.delenv("DK_HASH_LOG2")
+    monkeypatch.delenv("DK_GTABLE_LOG2")
     gpu2 = idx.search(Knn(10, 200), FullPrecision(), q)
     assert_same(gpu2, ref)
 
