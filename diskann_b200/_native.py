@@ -11,7 +11,8 @@ import os
 import threading
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "_lib", "libdiskann_b200.so")
+# DISKANN_B200_LIB selects another build of the same library (for example a profiling build).
+LIB_PATH = os.environ.get("DISKANN_B200_LIB") or os.path.join(_HERE, "_lib", "libdiskann_b200.so")
 
 # Every symbol include/diskann_b200.h declares (checked by the ABI test).
 EXPORTED_SYMBOLS = (

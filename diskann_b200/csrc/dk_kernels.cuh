@@ -52,6 +52,12 @@ constexpr uint32_t kIdMask = 0x7FFFFFFFu;
 constexpr uint32_t kFull = 0xFFFFFFFFu;
 constexpr int kCtaThreads = 128;
 
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
 // ----------------------------------------------------------------------------------------
 // Visited sets.
 // ----------------------------------------------------------------------------------------
@@ -96,70 +102,72 @@ struct BitmapSet {
   }
 };
 
-// Exact visited set in two levels: a small shared-memory hash takes the first `slimit` ids;
-// once it holds that many it stops accepting, and every later new id goes to a larger
-// open-addressing hash in global memory (one per warp).  The shared level never changes
-// after it fills, so "absent from the shared level" followed by a global probe is exact.
-// Ids reaching `insert` in one round are distinct (adjacency lists are de-duplicated when
-// the index is built and beam rows are filtered one after another).
-struct TwoLevelSet {
+// Exact visited set of one warp, in two levels: a small shared-memory hash takes the first
+// `slimit` ids; after it holds that many it never changes again, and every later new id goes
+// to a larger open-addressing hash in global memory owned by the warp.  Because the shared
+// level is frozen once full, "absent from the shared level" followed by a global probe is an
+// exact membership test.  The warp inserts up to 32 distinct ids at a time (adjacency lists
+// are de-duplicated when the index is built and beam rows are filtered one after another);
+// the counters are warp-uniform registers updated from ballots.
+struct WarpVisited {
   uint32_t* s;
   uint32_t smask, sshift, slimit;
-  uint32_t* scount;  // shared: ids accepted by the shared level (may overshoot slimit)
   uint32_t* g;
   uint32_t gmask, gshift;
-  uint32_t* gcount;  // shared: ids stored in the global level
+  uint32_t scount = 0;  // ids in the shared level
+  uint32_t gcount = 0;  // ids in the global level
 
-  __device__ void reset(uint32_t lane) const {
+  __device__ void reset(uint32_t lane) {
     for (uint32_t i = lane; i <= smask; i += 32u) s[i] = kEmpty;
-    if (lane == 0) {
-      *scount = 0u;
-      *gcount = 0u;
-    }
+    scount = 0u;
+    gcount = 0u;
   }
-  __device__ bool insert(uint32_t id) const {
+  // Every lane calls; lanes with `want` test-and-insert their `id`.  True if it was new.
+  __device__ bool insert(bool want, uint32_t id) {
     volatile uint32_t* vs = s;
+    bool present = false;
     uint32_t h = (id * 2654435761u) >> sshift;
-    while (true) {
-      const uint32_t cur = vs[h];
-      if (cur == id) return false;
-      if (cur == kEmpty) break;
-      h = (h + 1) & smask;
+    if (want) {
+      while (true) {
+        const uint32_t cur = vs[h];
+        if (cur == id) { present = true; break; }
+        if (cur == kEmpty) break;
+        h = (h + 1) & smask;
+      }
     }
-    if (*(volatile uint32_t*)scount < slimit && atomicAdd(scount, 1u) < slimit) {
-      // A slot of the shared level is reserved for this id: take the next empty one.
+    const bool absent = want && !present;
+    const uint32_t m = __ballot_sync(kFull, absent);
+    const uint32_t rank = __popc(m & lanemask_lt());
+    const uint32_t room = scount < slimit ? slimit - scount : 0u;
+    bool fresh = false;
+    if (absent && rank < room) {
+      // Take the first empty slot from the probe's end; other lanes only add other ids.
       while (atomicCAS(&s[h], kEmpty, id) != kEmpty) {
         do { h = (h + 1) & smask; } while (vs[h] != kEmpty);
       }
-      return true;
+      fresh = true;
     }
-    volatile uint32_t* vg = g;
-    uint32_t hg = ((id ^ 0x5bd1e995u) * 0x9E3779B1u) >> gshift;
-    while (true) {
-      const uint32_t cur = vg[hg];
-      if (cur == id) return false;
-      if (cur == kEmpty) {
-        const uint32_t old = atomicCAS(&g[hg], kEmpty, id);
-        if (old == kEmpty) {
-          atomicAdd(gcount, 1u);
-          return true;
+    scount += min((uint32_t)__popc(m), room);
+    const bool global = absent && rank >= room;
+    if (__any_sync(kFull, global)) {
+      if (global) {
+        uint32_t hg = ((id ^ 0x5bd1e995u) * 0x9E3779B1u) >> gshift;
+        while (true) {
+          const uint32_t old = atomicCAS(&g[hg], kEmpty, id);  // one round trip per step
+          if (old == kEmpty) { fresh = true; break; }
+          if (old == id) break;
+          hg = (hg + 1) & gmask;
         }
-        if (old == id) return false;
       }
-      hg = (hg + 1) & gmask;
+      gcount += __popc(__ballot_sync(kFull, global && fresh));
     }
+    return fresh;
   }
 };
 
 // ----------------------------------------------------------------------------------------
 // Small helpers.
 // ----------------------------------------------------------------------------------------
-
-__device__ __forceinline__ uint32_t lanemask_lt() {
-  uint32_t m;
-  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
-  return m;
-}
 
 // Exclusive prefix of a 0/1 flag over the block, in thread order; `total` = block sum.
 template <int NT>
@@ -883,7 +891,7 @@ __device__ void warp_post_process(const SearchParams& P, const State& S, uint32_
 // One query, run by one warp.  Writes the query's outputs and stats (or the spill flag).
 template <int METRIC, bool PQ, int DIM, int U>
 __device__ __forceinline__ void warp_query(const SearchParams& P, const State& S,
-                                           const TwoLevelSet& vset, uint32_t qid, uint32_t lane) {
+                                           WarpVisited& vset, uint32_t qid, uint32_t lane) {
   const float* qsrc = P.queries + (size_t)qid * P.qstride;
   const uint32_t dpad = (P.dim + 7u) & ~7u;
   for (uint32_t i = lane; i < dpad; i += 32u) S.q[i] = i < P.dim ? qsrc[i] : 0.0f;
@@ -898,9 +906,10 @@ __device__ __forceinline__ void warp_query(const SearchParams& P, const State& S
     return;
   }
   uint32_t size = 0, cursor = 0, cur = 0;
-  for (uint32_t s = lane; s < P.f; s += 32u) {
-    S.cand_id[s] = P.n + s;
-    vset.insert(P.n + s);
+  for (uint32_t s0 = 0; s0 < P.f; s0 += 32u) {
+    const uint32_t s = s0 + lane;
+    if (s < P.f) S.cand_id[s] = P.n + s;
+    vset.insert(s < P.f, P.n + s);
   }
   __syncwarp();
   warp_score<METRIC, PQ, DIM, U>(P, S, S.cand_id, S.cand_d, P.f, lane);
@@ -935,7 +944,7 @@ __device__ __forceinline__ void warp_query(const SearchParams& P, const State& S
     cursor = min(c, size);
     __syncwarp();
     // The global level must keep room for a whole hop going there; otherwise spill.
-    if (*(volatile uint32_t*)vset.gcount + nb * P.max_degree > P.gtable_limit) {
+    if (vset.gcount + nb * P.max_degree > P.gtable_limit) {
       if (lane == 0) P.stats[qid] = dk_search_stats{0u, 0u, 0u, kFlagSpilled};
       return;
     }
@@ -959,7 +968,7 @@ __device__ __forceinline__ void warp_query(const SearchParams& P, const State& S
         } else {
           id = t < deg ? __ldg(row + 1 + t) : 0u;
         }
-        const bool fresh = t < deg && vset.insert(id);
+        const bool fresh = vset.insert(t < deg, id);
         const uint32_t m = __ballot_sync(kFull, fresh);
         if (fresh) S.cand_id[count + __popc(m & lanemask_lt())] = id;
         count += __popc(m);
@@ -987,16 +996,14 @@ __global__ void __launch_bounds__(128) k_search_warp(const SearchParams P) {
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
   const uint32_t slot = blockIdx.x * (blockDim.x >> 5) + warp;
   const State S = carve(smem + (size_t)warp * P.warp_smem, P);
-  TwoLevelSet vset;
+  WarpVisited vset;
   vset.s = S.hash;
   vset.smask = (1u << P.hash_log2) - 1u;
   vset.sshift = 32u - P.hash_log2;
   vset.slimit = P.hash_limit;
-  vset.scount = &S.misc->scount;
   vset.g = P.gtable + ((size_t)slot << P.gtable_log2);
   vset.gmask = (1u << P.gtable_log2) - 1u;
   vset.gshift = 32u - P.gtable_log2;
-  vset.gcount = &S.misc->gcount;
   bool gdirty = true;  // the overflow table starts as uninitialised memory
   while (true) {
     uint32_t qid = 0;
@@ -1009,7 +1016,7 @@ __global__ void __launch_bounds__(128) k_search_warp(const SearchParams P) {
     }
     warp_query<METRIC, PQ, DIM, U>(P, S, vset, qid, lane);
     __syncwarp();
-    gdirty = *(volatile uint32_t*)vset.gcount != 0u;
+    gdirty = vset.gcount != 0u;
   }
 }
 
