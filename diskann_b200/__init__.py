@@ -8,7 +8,9 @@ either side of the path (synthetic inputs, graph construction, file formats).
 
 from .index import (  # noqa: F401
     ANNError,
+    BF16,
     DiskANNIndex,
+    FP8,
     FullPrecision,
     GpuProvider,
     Hybrid,
@@ -22,6 +24,6 @@ from .index import (  # noqa: F401
 )
 
 __all__ = [
-    "ANNError", "DiskANNIndex", "FullPrecision", "GpuProvider", "Hybrid", "Knn",
+    "ANNError", "BF16", "DiskANNIndex", "FP8", "FullPrecision", "GpuProvider", "Hybrid", "Knn",
     "KnnSearchError", "Metric", "PQData", "Quantized", "STATS_DTYPE", "Status",
 ]

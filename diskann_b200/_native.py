@@ -49,7 +49,12 @@ class IndexDesc(ctypes.Structure):
         ("pq_pivots", ctypes.c_void_p),
         ("pq_codes", ctypes.c_void_p),
         ("pq_code_stride", ctypes.c_uint64),
+        ("flags", ctypes.c_uint32),
     ]
+
+
+INDEX_BF16 = 1
+INDEX_FP8 = 2
 
 
 class IndexInfo(ctypes.Structure):

@@ -42,6 +42,9 @@ void free_index(dk_index* ix) {
   cudaFree(ix->pivots);
   cudaFree(ix->pivots_cm);
   cudaFree(ix->offsets);
+  cudaFree(ix->vec_bf16);
+  cudaFree(ix->vec_fp8);
+  cudaFree(ix->fp8_scale);
   if (ix->hint_host) cudaFreeHost(ix->hint_host);
   cudaSetDevice(prev);
   delete ix;
@@ -66,13 +69,17 @@ int32_t check_search_args(const dk_index* ix, int32_t strategy, uint32_t k, uint
   if (!ix) return fail(DK_ERR_INVALID_ARGUMENT, "index is null");
   const int32_t v = dk_knn_validate(k, l, beam);
   if (v != DK_OK) return v;
-  if (strategy < DK_STRATEGY_FULL_PRECISION || strategy > DK_STRATEGY_QUANTIZED)
+  if (strategy < DK_STRATEGY_FULL_PRECISION || strategy > DK_STRATEGY_FP8)
     return fail(DK_ERR_INVALID_ARGUMENT, "unknown strategy");
-  if (strategy != DK_STRATEGY_FULL_PRECISION) {
+  if (strategy == DK_STRATEGY_HYBRID || strategy == DK_STRATEGY_QUANTIZED) {
     if (ix->pq_chunks == 0) return fail(DK_ERR_NO_PQ, "index has no PQ data");
     if (ix->metric == DK_METRIC_COSINE)
       return fail(DK_ERR_UNSUPPORTED, "PQ traversal with the Cosine metric is not supported");
   }
+  if (strategy == DK_STRATEGY_BF16 && !ix->vec_bf16)
+    return fail(DK_ERR_NO_LOW_PRECISION, "index was created without DK_INDEX_BF16");
+  if (strategy == DK_STRATEGY_FP8 && !ix->vec_fp8)
+    return fail(DK_ERR_NO_LOW_PRECISION, "index was created without DK_INDEX_FP8");
   if (beam > 64) return fail(DK_ERR_UNSUPPORTED, "beam_width above 64 is not supported");
   if ((uint64_t)l + ix->f > 16384) return fail(DK_ERR_UNSUPPORTED, "L above 16383 is not supported");
   if (qstride < ix->dim) return fail(DK_ERR_DIMENSION_MISMATCH, "query stride below dim");
@@ -217,6 +224,8 @@ extern "C" int32_t dk_index_create(const dk_index_desc* d, int32_t device, dk_in
     if (e == cudaSuccess)
       e = upload(reinterpret_cast<void**>(&ix->offsets), d->pq_offsets, (d->pq_chunks + 1) * sizeof(uint32_t));
   }
+  if (e == cudaSuccess && (d->flags & (DK_INDEX_BF16 | DK_INDEX_FP8)))
+    e = dk_build_low_precision(ix, d->flags);
   if (e == cudaSuccess) {
     e = cudaHostAlloc(reinterpret_cast<void**>(&ix->hint_host), 2 * sizeof(uint32_t), cudaHostAllocMapped);
     if (e == cudaSuccess) {

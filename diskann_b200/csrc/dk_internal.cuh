@@ -26,6 +26,11 @@ struct dk_index {
   float* pivots = nullptr;
   float* pivots_cm = nullptr;  // chunk-major copy: chunk m, centre c -> len_m floats
   uint32_t* offsets = nullptr;
+  // Low-precision copies: rows of lp_stride elements (a multiple of 16, zero padded).
+  uint16_t* vec_bf16 = nullptr;   // BF16 bit patterns
+  uint8_t* vec_fp8 = nullptr;     // FP8-E4M3, value = fp8 * fp8_scale[row]
+  float* fp8_scale = nullptr;
+  uint32_t lp_stride = 0;
   uint64_t bytes = 0;
   // Visited-set sizing hint in mapped pinned host memory: word 0 = largest
   // cmps * 256 / (L + F) seen by kernels since the last launch read it, word 1 = the value the
@@ -42,6 +47,10 @@ struct SearchParams {
   const float* pivots;
   const float* pivots_cm;
   const uint32_t* offsets;
+  const uint16_t* vec_bf16;
+  const uint8_t* vec_fp8;
+  const float* fp8_scale;
+  uint32_t lp_stride;
   uint32_t n, f, dim, vstride, astride, max_degree, cstride, pq_chunks;
   const float* queries;
   uint64_t qstride;
@@ -74,8 +83,33 @@ struct SearchParams {
 
 constexpr uint32_t kFlagSpilled = 1u;
 
+// How candidates are scored during traversal.
+constexpr int kModeFP32 = 0;
+constexpr int kModePQ = 1;
+constexpr int kModeBF16 = 2;
+constexpr int kModeFP8 = 3;
+
+inline int mode_of_strategy(int32_t strategy) {
+  switch (strategy) {
+    case DK_STRATEGY_HYBRID:
+    case DK_STRATEGY_QUANTIZED: return kModePQ;
+    case DK_STRATEGY_BF16: return kModeBF16;
+    case DK_STRATEGY_FP8: return kModeFP8;
+    default: return kModeFP32;
+  }
+}
+
+// Strategies whose post-processing re-ranks the queue with exact FP32 distances.
+__host__ __device__ inline bool strategy_reranks(int32_t strategy) {
+  return strategy == DK_STRATEGY_HYBRID || strategy == DK_STRATEGY_BF16 ||
+         strategy == DK_STRATEGY_FP8;
+}
+
 // Thread-local error reporting for the C ABI.
 void dk_set_error(int32_t status, const std::string& msg);
+
+// Derive the low-precision copies requested by `flags` from the index's FP32 rows.
+cudaError_t dk_build_low_precision(dk_index* ix, uint32_t flags);
 
 // Launch the search (first pass + spill pass) on `stream`.  Parameters are validated by
 // the caller.

@@ -37,6 +37,8 @@
 // scored and counted but never inserted (queue.rs:131-135).
 #pragma once
 
+#include <cuda_fp16.h>
+#include <cuda_fp8.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -247,14 +249,32 @@ __device__ __forceinline__ void subgroup_distances(const float* const (&rows)[U]
   float acc[U][4];
 #pragma unroll
   for (int u = 0; u < U; ++u) acc[u][0] = acc[u][1] = acc[u][2] = acc[u][3] = 0.0f;
+  if (DIM > 0 && DIM % 32 == 0 && DIM / 32 * U <= 16) {
+    // Every 16-byte piece of the U rows is requested before the first FMA, so one round
+    // costs one memory latency.  The FMAs then run in the reference's block order.
+    constexpr int NB = DIM > 0 ? DIM / 32 : 1;
+    float4 v[U][NB];
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+      for (int b = 0; b < NB; ++b)
+        v[u][b] = __ldg(reinterpret_cast<const float4*>(rows[u]) + 8 * b + s);
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+      const float4 a = q4[8 * b + s];
+#pragma unroll
+      for (int u = 0; u < U; ++u) acc4<METRIC>(a, v[u][b], acc[u]);
+    }
+  } else {
 #pragma unroll 4
-  for (uint32_t base = 4u * s; base < full; base += 32u) {
-    const float4 a = q4[base >> 2];
-    float4 v[U];
+    for (uint32_t base = 4u * s; base < full; base += 32u) {
+      const float4 a = q4[base >> 2];
+      float4 v[U];
 #pragma unroll
-    for (int u = 0; u < U; ++u) v[u] = __ldg(reinterpret_cast<const float4*>(rows[u]) + (base >> 2));
+      for (int u = 0; u < U; ++u) v[u] = __ldg(reinterpret_cast<const float4*>(rows[u]) + (base >> 2));
 #pragma unroll
-    for (int u = 0; u < U; ++u) acc4<METRIC>(a, v[u], acc[u]);
+      for (int u = 0; u < U; ++u) acc4<METRIC>(a, v[u], acc[u]);
+    }
   }
 #pragma unroll
   for (int u = 0; u < U; ++u)
@@ -390,6 +410,120 @@ __device__ __forceinline__ void score_fp(const SearchParams& P, const float* q,
 #pragma unroll
       for (int u = 0; u < U; ++u)
         if (idx[u] < count) d[idx[u]] = out[u];
+    }
+  }
+}
+
+// Low-precision candidate scoring (BF16 rows, or FP8-E4M3 rows times a per-row scale), FP32
+// accumulation.  Lane s of a subgroup reads 16-byte pieces s, s+8, s+16, ... of each row
+// (8 BF16 or 16 FP8 elements per piece); partial sums meet in a butterfly over the 8 lanes.
+// These distances steer the traversal only: the strategies re-rank with exact FP32 rows.
+__device__ __forceinline__ void bf16x8(const uint4 w, float (&x)[8]) {
+  const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    x[2 * i] = __uint_as_float(ws[i] << 16);
+    x[2 * i + 1] = __uint_as_float(ws[i] & 0xFFFF0000u);
+  }
+}
+
+__device__ __forceinline__ void fp8x16(const uint4 w, float (&x)[16]) {
+  const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const __nv_fp8x2_storage_t pair = (__nv_fp8x2_storage_t)((ws[i] >> (16 * h)) & 0xFFFFu);
+      const __half2_raw hr = __nv_cvt_fp8x2_to_halfraw2(pair, __NV_E4M3);
+      const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&hr));
+      x[4 * i + 2 * h] = f.x;
+      x[4 * i + 2 * h + 1] = f.y;
+    }
+  }
+}
+
+template <int METRIC, int MODE, int U>
+__device__ __forceinline__ void score_lp(const SearchParams& P, const float* q, const uint32_t* ids,
+                                         float* d, uint32_t count, uint32_t sg, uint32_t nsub,
+                                         uint32_t s, unsigned gmask) {
+  constexpr uint32_t kPer = MODE == kModeBF16 ? 8u : 16u;  // elements per 16-byte piece
+  const uint32_t pieces = P.lp_stride / kPer;
+  const uint32_t row_bytes = P.lp_stride * (MODE == kModeBF16 ? 2u : 1u);
+  const unsigned char* base = MODE == kModeBF16
+                                  ? reinterpret_cast<const unsigned char*>(P.vec_bf16)
+                                  : reinterpret_cast<const unsigned char*>(P.vec_fp8);
+  const uint32_t step = nsub * U;
+  for (uint32_t b0 = 0; b0 < count; b0 += step) {
+    const uint4* rows[U];
+    uint32_t idx[U], rid[U];
+    float acc[U], yy[U], qq = 0.0f;
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      idx[u] = b0 + sg + u * nsub;
+      rid[u] = ids[idx[u] < count ? idx[u] : count - 1];
+      rows[u] = reinterpret_cast<const uint4*>(base + (size_t)rid[u] * row_bytes);
+      acc[u] = 0.0f;
+      yy[u] = 0.0f;
+    }
+    float scale[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) scale[u] = MODE == kModeFP8 ? __ldg(P.fp8_scale + rid[u]) : 1.0f;
+    for (uint32_t p = s; p < pieces; p += 8u) {
+      uint4 w[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) w[u] = __ldg(rows[u] + p);
+      float qv[kPer];
+      const float4* q4 = reinterpret_cast<const float4*>(q + p * kPer);
+#pragma unroll
+      for (uint32_t i = 0; i < kPer / 4; ++i) {
+        const float4 t = q4[i];
+        qv[4 * i] = t.x; qv[4 * i + 1] = t.y; qv[4 * i + 2] = t.z; qv[4 * i + 3] = t.w;
+      }
+      if (METRIC == DK_METRIC_COSINE) {
+#pragma unroll
+        for (uint32_t i = 0; i < kPer; ++i) qq = __fmaf_rn(qv[i], qv[i], qq);
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        float x[kPer];
+        if (MODE == kModeBF16) bf16x8(w[u], *reinterpret_cast<float(*)[8]>(x));
+        else fp8x16(w[u], *reinterpret_cast<float(*)[16]>(x));
+#pragma unroll
+        for (uint32_t i = 0; i < kPer; ++i) {
+          if (METRIC == DK_METRIC_L2) {
+            const float c = qv[i] - scale[u] * x[i];
+            acc[u] = __fmaf_rn(c, c, acc[u]);
+          } else {
+            acc[u] = __fmaf_rn(qv[i], x[i], acc[u]);
+            if (METRIC == DK_METRIC_COSINE) yy[u] = __fmaf_rn(x[i], x[i], yy[u]);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int o = 1; o < 8; o <<= 1) {
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        acc[u] += __shfl_xor_sync(gmask, acc[u], o, 8);
+        if (METRIC == DK_METRIC_COSINE) yy[u] += __shfl_xor_sync(gmask, yy[u], o, 8);
+      }
+      if (METRIC == DK_METRIC_COSINE) qq += __shfl_xor_sync(gmask, qq, o, 8);
+    }
+    if (s == 0) {
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (idx[u] >= count) continue;
+        float r;
+        if (METRIC == DK_METRIC_L2) r = acc[u];
+        else if (METRIC == DK_METRIC_INNER_PRODUCT) r = -scale[u] * acc[u];
+        else if (METRIC == DK_METRIC_COSINE_NORMALIZED) r = 1.0f - scale[u] * acc[u];
+        else {
+          const float den = sqrtf(qq) * sqrtf(yy[u]);
+          r = (qq < 1.17549435e-38f || yy[u] < 1.17549435e-38f) ? 1.0f
+              : 1.0f - fmaxf(-1.0f, fminf(1.0f, acc[u] / den));
+        }
+        d[idx[u]] = r;
+      }
     }
   }
 }
@@ -536,16 +670,19 @@ __device__ __forceinline__ void record_hint(const SearchParams& P, uint32_t cmps
 // CTA-per-query kernel.
 // ========================================================================================
 
-template <int NT, int METRIC, bool PQ, int DIM>
+template <int NT, int METRIC, int MODE, int DIM>
 __device__ __forceinline__ void cta_score(const SearchParams& P, const State& S, const uint32_t* ids,
                                           float* d, uint32_t count) {
   const uint32_t tid = threadIdx.x;
-  if (PQ) {
+  if (MODE == kModePQ) {
     for (uint32_t i = tid; i < count; i += NT)
       d[i] = pq_distance(P.codes + (size_t)ids[i] * P.cstride, S.table, P.pq_chunks);
   } else {
     const unsigned gmask = 0xFFu << (8u * ((tid & 31u) >> 3));
-    score_fp<METRIC, DIM, 1>(P, S.q, ids, d, count, tid >> 3, NT / 8, tid & 7u, gmask);
+    if (MODE == kModeFP32)
+      score_fp<METRIC, DIM, 1>(P, S.q, ids, d, count, tid >> 3, NT / 8, tid & 7u, gmask);
+    else
+      score_lp<METRIC, MODE, 1>(P, S.q, ids, d, count, tid >> 3, NT / 8, tid & 7u, gmask);
   }
 }
 
@@ -618,18 +755,18 @@ __device__ void cta_post_process(const SearchParams& P, const State& S, uint32_t
     uint32_t total;
     const uint32_t pos = base + block_scan<NT>(keep, M->warp_sums, total);
     if (keep) {
-      if (P.strategy == DK_STRATEGY_HYBRID) S.cand_id[pos] = id;
+      if (strategy_reranks(P.strategy)) S.cand_id[pos] = id;
       else if (pos < P.k) { out_ids[pos] = id; out_d[pos] = qd[i]; }
     }
     base += total;
   }
-  if (P.strategy != DK_STRATEGY_HYBRID) {
+  if (!strategy_reranks(P.strategy)) {
     written = min(base, P.k);
   } else {
     // Rerank (inmem/full_precision.rs:357-404): exact distances, stable sort, first k.
     const uint32_t count = base;
     __syncthreads();
-    cta_score<NT, METRIC, false, DIM>(P, S, S.cand_id, S.cand_d, count);
+    cta_score<NT, METRIC, kModeFP32, DIM>(P, S, S.cand_id, S.cand_d, count);
     __syncthreads();
     for (uint32_t i = tid; i < count; i += NT) {
       const float d = S.cand_d[i];
@@ -652,20 +789,20 @@ __device__ void cta_post_process(const SearchParams& P, const State& S, uint32_t
 }
 
 // The whole search of one query by one CTA.  Returns false if the visited set overflowed.
-template <int NT, int METRIC, bool PQ, int DIM, class VSet>
+template <int NT, int METRIC, int MODE, int DIM, class VSet>
 __device__ bool cta_search(const SearchParams& P, const State& S, const VSet& vset, uint32_t qid,
                            uint32_t& cmps_out, uint32_t& hops_out) {
   const uint32_t tid = threadIdx.x;
   Misc* M = S.misc;
   const float* qsrc = P.queries + (size_t)qid * P.qstride;
-  const uint32_t dpad = (P.dim + 7u) & ~7u;
+  const uint32_t dpad = (P.dim + 15u) & ~15u;  // zero padded: FP8 pieces hold 16 elements
   for (uint32_t i = tid; i < dpad; i += NT) S.q[i] = i < P.dim ? qsrc[i] : 0.0f;
   vset.clear(tid, NT);
   if (tid == 0) {
     M->size = M->cursor = M->cur = M->inserted = M->overflow = M->nvalid = 0;
   }
   __syncthreads();
-  if (PQ) {
+  if (MODE == kModePQ) {
     build_table<METRIC>(P, S.q, S.table, tid, NT);
     __syncthreads();
   }
@@ -677,7 +814,7 @@ __device__ bool cta_search(const SearchParams& P, const State& S, const VSet& vs
   }
   if (tid == 0) M->inserted = P.f;
   __syncthreads();
-  cta_score<NT, METRIC, PQ, DIM>(P, S, S.cand_id, S.cand_d, P.f);
+  cta_score<NT, METRIC, MODE, DIM>(P, S, S.cand_id, S.cand_d, P.f);
   __syncthreads();
   cta_merge<NT>(P, S, P.f);
   uint32_t cmps = P.f, hops = 0;
@@ -720,7 +857,7 @@ __device__ bool cta_search(const SearchParams& P, const State& S, const VSet& vs
     }
     if (tid == 0) M->inserted += count;
     __syncthreads();
-    cta_score<NT, METRIC, PQ, DIM>(P, S, S.cand_id, S.cand_d, count);
+    cta_score<NT, METRIC, MODE, DIM>(P, S, S.cand_id, S.cand_d, count);
     __syncthreads();
     cta_merge<NT>(P, S, count);
     cmps += count;
@@ -731,7 +868,7 @@ __device__ bool cta_search(const SearchParams& P, const State& S, const VSet& vs
   return true;
 }
 
-template <int NT, int METRIC, bool PQ, int DIM>
+template <int NT, int METRIC, int MODE, int DIM>
 __global__ void __launch_bounds__(NT) k_search_cta(const SearchParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
   const State S = carve(smem, P);
@@ -739,7 +876,7 @@ __global__ void __launch_bounds__(NT) k_search_cta(const SearchParams P) {
   const uint32_t qid = blockIdx.x;
   if (qid >= P.nq) return;
   uint32_t cmps = 0, hops = 0;
-  if (!cta_search<NT, METRIC, PQ, DIM>(P, S, vset, qid, cmps, hops)) {
+  if (!cta_search<NT, METRIC, MODE, DIM>(P, S, vset, qid, cmps, hops)) {
     if (threadIdx.x == 0) P.stats[qid] = dk_search_stats{0u, 0u, 0u, kFlagSpilled};
     return;
   }
@@ -752,7 +889,7 @@ __global__ void __launch_bounds__(NT) k_search_cta(const SearchParams P) {
 }
 
 // Spill pass: each CTA owns one bitmap slice and re-runs the queries the first pass flagged.
-template <int NT, int METRIC, bool PQ, int DIM>
+template <int NT, int METRIC, int MODE, int DIM>
 __global__ void __launch_bounds__(NT) k_search_spill(const SearchParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
   const State S = carve(smem, P);
@@ -761,7 +898,7 @@ __global__ void __launch_bounds__(NT) k_search_spill(const SearchParams P) {
     if (!(P.stats[qid].flags & kFlagSpilled)) continue;
     __syncthreads();
     uint32_t cmps = 0, hops = 0;
-    cta_search<NT, METRIC, PQ, DIM>(P, S, vset, qid, cmps, hops);
+    cta_search<NT, METRIC, MODE, DIM>(P, S, vset, qid, cmps, hops);
     cta_post_process<NT, METRIC, DIM>(P, S, qid);
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -823,16 +960,19 @@ __device__ __forceinline__ void warp_merge(const SearchParams& P, const State& S
   __syncwarp();
 }
 
-template <int METRIC, bool PQ, int DIM, int U>
+template <int METRIC, int MODE, int DIM, int U>
 __device__ __forceinline__ void warp_score(const SearchParams& P, const State& S,
                                            const uint32_t* ids, float* d, uint32_t count,
                                            uint32_t lane) {
-  if (PQ) {
+  if (MODE == kModePQ) {
     for (uint32_t i = lane; i < count; i += 32u)
       d[i] = pq_distance(P.codes + (size_t)ids[i] * P.cstride, S.table, P.pq_chunks);
   } else {
     const unsigned gmask = 0xFFu << (8u * (lane >> 3));
-    score_fp<METRIC, DIM, U>(P, S.q, ids, d, count, lane >> 3, 4u, lane & 7u, gmask);
+    if (MODE == kModeFP32)
+      score_fp<METRIC, DIM, U>(P, S.q, ids, d, count, lane >> 3, 4u, lane & 7u, gmask);
+    else
+      score_lp<METRIC, MODE, 2>(P, S.q, ids, d, count, lane >> 3, 4u, lane & 7u, gmask);
   }
   __syncwarp();
 }
@@ -845,7 +985,7 @@ __device__ void warp_post_process(const SearchParams& P, const State& S, uint32_
   const uint32_t* qi = S.qi[cur];
   uint32_t* out_ids = P.out_ids + (size_t)qid * P.k;
   float* out_d = P.out_dists + (size_t)qid * P.k;
-  const bool hybrid = P.strategy == DK_STRATEGY_HYBRID;
+  const bool hybrid = strategy_reranks(P.strategy);
   uint32_t base = 0;
   for (uint32_t t0 = 0; t0 < size; t0 += 32u) {
     if (!hybrid && base >= P.k) break;
@@ -867,7 +1007,7 @@ __device__ void warp_post_process(const SearchParams& P, const State& S, uint32_
     // Rerank (inmem/full_precision.rs:357-404): exact distances, stable sort, first k.
     const uint32_t count = base;
     __syncwarp();
-    warp_score<METRIC, false, DIM, U>(P, S, S.cand_id, S.cand_d, count, lane);
+    warp_score<METRIC, kModeFP32, DIM, U>(P, S, S.cand_id, S.cand_d, count, lane);
     for (uint32_t i = lane; i < count; i += 32u) {
       const float d = S.cand_d[i];
       const bool dn = d != d;
@@ -889,15 +1029,15 @@ __device__ void warp_post_process(const SearchParams& P, const State& S, uint32_
 }
 
 // One query, run by one warp.  Writes the query's outputs and stats (or the spill flag).
-template <int METRIC, bool PQ, int DIM, int U>
+template <int METRIC, int MODE, int DIM, int U>
 __device__ __forceinline__ void warp_query(const SearchParams& P, const State& S,
                                            WarpVisited& vset, uint32_t qid, uint32_t lane) {
   const float* qsrc = P.queries + (size_t)qid * P.qstride;
-  const uint32_t dpad = (P.dim + 7u) & ~7u;
+  const uint32_t dpad = (P.dim + 15u) & ~15u;  // zero padded: FP8 pieces hold 16 elements
   for (uint32_t i = lane; i < dpad; i += 32u) S.q[i] = i < P.dim ? qsrc[i] : 0.0f;
   vset.reset(lane);
   __syncwarp();
-  if (PQ) {
+  if (MODE == kModePQ) {
     build_table<METRIC>(P, S.q, S.table, lane, 32u);
     __syncwarp();
   }
@@ -912,7 +1052,7 @@ __device__ __forceinline__ void warp_query(const SearchParams& P, const State& S
     vset.insert(s < P.f, P.n + s);
   }
   __syncwarp();
-  warp_score<METRIC, PQ, DIM, U>(P, S, S.cand_id, S.cand_d, P.f, lane);
+  warp_score<METRIC, MODE, DIM, U>(P, S, S.cand_id, S.cand_d, P.f, lane);
   warp_merge(P, S, P.f, lane, size, cursor, cur);
   uint32_t cmps = P.f, hops = 0;
   uint32_t* beam = S.misc->beam;
@@ -975,7 +1115,7 @@ __device__ __forceinline__ void warp_query(const SearchParams& P, const State& S
       }
     }
     __syncwarp();
-    warp_score<METRIC, PQ, DIM, U>(P, S, S.cand_id, S.cand_d, count, lane);
+    warp_score<METRIC, MODE, DIM, U>(P, S, S.cand_id, S.cand_d, count, lane);
     warp_merge(P, S, count, lane, size, cursor, cur);
     cmps += count;
     hops += nb;
@@ -990,7 +1130,7 @@ __device__ __forceinline__ void warp_query(const SearchParams& P, const State& S
 
 // Persistent grid: every warp owns a shared-memory slice and a global overflow table and
 // takes queries from a work counter until the batch is done.
-template <int METRIC, bool PQ, int DIM, int U>
+template <int METRIC, int MODE, int DIM, int U>
 __global__ void __launch_bounds__(128) k_search_warp(const SearchParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
@@ -1014,7 +1154,7 @@ __global__ void __launch_bounds__(128) k_search_warp(const SearchParams P) {
       for (uint32_t i = lane; i <= vset.gmask; i += 32u) vset.g[i] = kEmpty;
       __syncwarp();
     }
-    warp_query<METRIC, PQ, DIM, U>(P, S, vset, qid, lane);
+    warp_query<METRIC, MODE, DIM, U>(P, S, vset, qid, lane);
     __syncwarp();
     gdirty = vset.gcount != 0u;
   }
@@ -1033,54 +1173,78 @@ struct LaunchPlan {
   uint32_t warps_per_cta;
   uint32_t grid;       // warp kernel: persistent grid size
   uint32_t spill_ctas;
+  uint32_t score_u;    // warp kernel, D <= 128: rows per subgroup per round (2 or 4)
   bool query_only;     // warp kernel: only report `blocks_per_sm` for `warps_per_cta`
   int blocks_per_sm;
 };
 
-template <int METRIC, bool PQ, int DIM>
+template <int METRIC, int MODE, int DIM, int U>
+cudaError_t launch_warp(LaunchPlan& L, cudaStream_t stream) {
+  auto k1 = k_search_warp<METRIC, MODE, DIM, U>;
+  const uint32_t bytes = L.p1.warp_smem * L.warps_per_cta;
+  cudaError_t e = cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e != cudaSuccess) return e;
+  if (L.query_only)
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&L.blocks_per_sm, k1, 32 * L.warps_per_cta,
+                                                         bytes);
+  k1<<<L.grid, 32 * L.warps_per_cta, bytes, stream>>>(L.p1);
+  return cudaGetLastError();
+}
+
+template <int METRIC, int MODE, int DIM>
 cudaError_t launch_variant(LaunchPlan& L, cudaStream_t stream) {
   cudaError_t e;
-  constexpr int U = (DIM > 0 && DIM <= 128) ? 2 : 1;
   if (L.kind == KernelKind::kWarp) {
-    auto k1 = k_search_warp<METRIC, PQ, DIM, U>;
-    const uint32_t bytes = L.p1.warp_smem * L.warps_per_cta;
-    e = cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    if (e != cudaSuccess) return e;
-    if (L.query_only) {
-      return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&L.blocks_per_sm, k1,
-                                                           32 * L.warps_per_cta, bytes);
-    }
-    k1<<<L.grid, 32 * L.warps_per_cta, bytes, stream>>>(L.p1);
+    // Rows scored together per 8-lane subgroup: more rows in flight per round for narrow rows.
+    if (DIM > 0 && DIM <= 128 && L.score_u >= 4) e = launch_warp<METRIC, MODE, DIM, 4>(L, stream);
+    else if (DIM > 0 && DIM <= 128) e = launch_warp<METRIC, MODE, DIM, 2>(L, stream);
+    else e = launch_warp<METRIC, MODE, DIM, 1>(L, stream);
+    if (e != cudaSuccess || L.query_only) return e;
   } else {
-    auto k1 = k_search_cta<kCtaThreads, METRIC, PQ, DIM>;
+    auto k1 = k_search_cta<kCtaThreads, METRIC, MODE, DIM>;
     e = cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.p1.smem_bytes);
     if (e != cudaSuccess) return e;
     k1<<<L.p1.nq, kCtaThreads, L.p1.smem_bytes, stream>>>(L.p1);
   }
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  auto k2 = k_search_spill<kCtaThreads, METRIC, PQ, DIM>;
+  auto k2 = k_search_spill<kCtaThreads, METRIC, MODE, DIM>;
   e = cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.p2.smem_bytes);
   if (e != cudaSuccess) return e;
   k2<<<L.spill_ctas, kCtaThreads, L.p2.smem_bytes, stream>>>(L.p2);
   return cudaGetLastError();
 }
 
-template <int METRIC, bool PQ>
+template <int METRIC, int MODE>
 cudaError_t launch_dims(LaunchPlan& L, cudaStream_t stream) {
   switch (L.p1.dim) {
-    case 96: return launch_variant<METRIC, PQ, 96>(L, stream);
-    case 128: return launch_variant<METRIC, PQ, 128>(L, stream);
-    case 384: return launch_variant<METRIC, PQ, 384>(L, stream);
-    case 768: return launch_variant<METRIC, PQ, 768>(L, stream);
-    default: return launch_variant<METRIC, PQ, 0>(L, stream);
+    case 96: return launch_variant<METRIC, MODE, 96>(L, stream);
+    case 128: return launch_variant<METRIC, MODE, 128>(L, stream);
+    case 384: return launch_variant<METRIC, MODE, 384>(L, stream);
+    case 768: return launch_variant<METRIC, MODE, 768>(L, stream);
+    default: return launch_variant<METRIC, MODE, 0>(L, stream);
   }
 }
 
 }  // namespace dk
 
 // Per-metric entry points (one translation unit each, compiled in parallel).
-cudaError_t dk_launch_l2(dk::LaunchPlan& L, bool pq, cudaStream_t stream);
-cudaError_t dk_launch_ip(dk::LaunchPlan& L, bool pq, cudaStream_t stream);
-cudaError_t dk_launch_cosine(dk::LaunchPlan& L, bool pq, cudaStream_t stream);
-cudaError_t dk_launch_cosine_normalized(dk::LaunchPlan& L, bool pq, cudaStream_t stream);
+cudaError_t dk_launch_l2(dk::LaunchPlan& L, int mode, cudaStream_t stream);
+cudaError_t dk_launch_ip(dk::LaunchPlan& L, int mode, cudaStream_t stream);
+cudaError_t dk_launch_cosine(dk::LaunchPlan& L, int mode, cudaStream_t stream);
+cudaError_t dk_launch_cosine_normalized(dk::LaunchPlan& L, int mode, cudaStream_t stream);
+
+namespace dk {
+// All scoring modes of one metric (PQ traversal is not offered with the Cosine metric).
+template <int METRIC>
+cudaError_t launch_modes(LaunchPlan& L, int mode, cudaStream_t stream) {
+  switch (mode) {
+    case kModePQ:
+      if (METRIC != DK_METRIC_COSINE) return launch_dims<METRIC, kModePQ>(L, stream);
+      return cudaErrorInvalidValue;
+    case kModeBF16: return launch_dims<METRIC, kModeBF16>(L, stream);
+    case kModeFP8: return launch_dims<METRIC, kModeFP8>(L, stream);
+    default: return launch_dims<METRIC, kModeFP32>(L, stream);
+  }
+}
+}  // namespace dk

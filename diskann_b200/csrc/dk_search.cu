@@ -25,7 +25,7 @@ uint32_t plan_query_smem(SearchParams& P, bool pq, bool with_hash) {
     off = align_up(off + bytes, 16);
     return o;
   };
-  P.off_query = take(align_up(P.dim, 8) * 4);
+  P.off_query = take(align_up(P.dim, 16) * 4);
   P.off_table = take(pq ? P.pq_chunks * 256u * 4u : 0u);
   P.off_qd0 = take(P.cap * 4);
   P.off_qi0 = take(P.cap * 4);
@@ -52,12 +52,12 @@ uint32_t log2_at_least(double x, uint32_t lo, uint32_t hi) {
   return l;
 }
 
-cudaError_t dispatch(int32_t metric, dk::LaunchPlan& L, bool pq, cudaStream_t stream) {
+cudaError_t dispatch(int32_t metric, dk::LaunchPlan& L, int mode, cudaStream_t stream) {
   switch (metric) {
-    case DK_METRIC_L2: return dk_launch_l2(L, pq, stream);
-    case DK_METRIC_INNER_PRODUCT: return dk_launch_ip(L, pq, stream);
-    case DK_METRIC_COSINE: return dk_launch_cosine(L, pq, stream);
-    default: return dk_launch_cosine_normalized(L, pq, stream);
+    case DK_METRIC_L2: return dk_launch_l2(L, mode, stream);
+    case DK_METRIC_INNER_PRODUCT: return dk_launch_ip(L, mode, stream);
+    case DK_METRIC_COSINE: return dk_launch_cosine(L, mode, stream);
+    default: return dk_launch_cosine_normalized(L, mode, stream);
   }
 }
 
@@ -73,7 +73,8 @@ int32_t dk_launch_search(const dk_index* ix, int32_t strategy, const float* quer
                          uint32_t* ids, float* dists, dk_search_stats* stats,
                          cudaStream_t stream) {
   if (nq == 0) return DK_OK;
-  const bool pq = strategy != DK_STRATEGY_FULL_PRECISION;
+  const int mode = mode_of_strategy(strategy);
+  const bool pq = mode == kModePQ;
   SearchParams P{};
   P.vectors = ix->vectors;
   P.adj = ix->adj;
@@ -81,6 +82,10 @@ int32_t dk_launch_search(const dk_index* ix, int32_t strategy, const float* quer
   P.pivots = ix->pivots;
   P.pivots_cm = ix->pivots_cm;
   P.offsets = ix->offsets;
+  P.vec_bf16 = ix->vec_bf16;
+  P.vec_fp8 = ix->vec_fp8;
+  P.fp8_scale = ix->fp8_scale;
+  P.lp_stride = ix->lp_stride;
   P.n = ix->n;
   P.f = ix->f;
   P.dim = ix->dim;
@@ -134,6 +139,7 @@ int32_t dk_launch_search(const dk_index* ix, int32_t strategy, const float* quer
   if (kenv && !strcmp(kenv, "cta")) warp = false;
 
   dk::LaunchPlan L{};
+  L.score_u = env_u32("DK_SCORE_U", 2);
   uint64_t gtable_bytes = 0;
   cudaError_t e = cudaSuccess;
   if (warp) {
@@ -160,9 +166,10 @@ int32_t dk_launch_search(const dk_index* ix, int32_t strategy, const float* quer
       dk::LaunchPlan Q{};
       Q.kind = dk::KernelKind::kWarp;
       Q.p1 = P;
+      Q.score_u = L.score_u;
       Q.warps_per_cta = wpc;
       Q.query_only = true;
-      e = dispatch(ix->metric, Q, pq, stream);
+      e = dispatch(ix->metric, Q, mode, stream);
       if (e != cudaSuccess) {
         dk_set_error(DK_ERR_CUDA, std::string("occupancy query: ") + cudaGetErrorString(e));
         return DK_ERR_CUDA;
@@ -219,7 +226,7 @@ int32_t dk_launch_search(const dk_index* ix, int32_t strategy, const float* quer
   L.p1 = P;
   L.p2 = P2;
   L.spill_ctas = spill_ctas;
-  if (e == cudaSuccess) e = dispatch(ix->metric, L, pq, stream);
+  if (e == cudaSuccess) e = dispatch(ix->metric, L, mode, stream);
   cudaFreeAsync(scratch, stream);
   if (e != cudaSuccess) {
     dk_set_error(DK_ERR_CUDA, std::string("search launch: ") + cudaGetErrorString(e));

@@ -1,7 +1,6 @@
-// Kernel instantiations for one metric (DK_METRIC_COSINE); see dk_kernels.cuh.
+// Kernel instantiations for one metric (DK_METRIC_COSINE), all scoring modes; see dk_kernels.cuh.
 #include "dk_kernels.cuh"
 
-cudaError_t dk_launch_cosine(dk::LaunchPlan& L, bool pq, cudaStream_t stream) {
-  (void)pq;
-  return dk::launch_dims<DK_METRIC_COSINE, false>(L, stream);
+cudaError_t dk_launch_cosine(dk::LaunchPlan& L, int mode, cudaStream_t stream) {
+  return dk::launch_modes<DK_METRIC_COSINE>(L, mode, stream);
 }

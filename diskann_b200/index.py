@@ -54,6 +54,7 @@ class Status(enum.IntEnum):
     ADMISSION = 13
     CANCELLED = 14
     NOT_FOUND = 15
+    NO_LOW_PRECISION = 16
 
 
 class ANNError(RuntimeError):
@@ -124,6 +125,20 @@ class Quantized(_Strategy):
     code = 2
 
 
+class BF16(_Strategy):
+    """Traversal scored from BF16 rows (FP32 accumulation); FilterStartPoints + exact FP32
+    Rerank.  Needs a provider created with ``low_precision=("bf16",)``."""
+
+    code = 3
+
+
+class FP8(_Strategy):
+    """Traversal scored from FP8-E4M3 rows with a per-vector FP32 scale (FP32 accumulation);
+    FilterStartPoints + exact FP32 Rerank.  Needs ``low_precision=("fp8",)``."""
+
+    code = 4
+
+
 @dataclass
 class PQData:
     """Product quantisation schema and codes (FixedChunkPQTable layout)."""
@@ -141,7 +156,7 @@ class GpuProvider:
     """
 
     def __init__(self, vectors, adjacency, degrees, num_points: int, metric=Metric.L2,
-                 pq: PQData | None = None, device: int = 0):
+                 pq: PQData | None = None, device: int = 0, low_precision=()):
         L = _native.load()
         vectors = np.ascontiguousarray(vectors, dtype=np.float32)
         adjacency = np.ascontiguousarray(adjacency, dtype=np.uint32)
@@ -157,6 +172,10 @@ class GpuProvider:
         d.adjacency_stride = adjacency.shape[1]
         d.degrees = degrees.ctypes.data
         d.max_degree = adjacency.shape[1]
+        flags = 0
+        for lp in low_precision:
+            flags |= {"bf16": _native.INDEX_BF16, "fp8": _native.INDEX_FP8}[lp]
+        d.flags = flags
         keep = [vectors, adjacency, degrees]
         if pq is not None:
             off = np.ascontiguousarray(pq.offsets, dtype=np.uint32)

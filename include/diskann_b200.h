@@ -54,7 +54,17 @@ enum dk_strategy {
   DK_STRATEGY_FULL_PRECISION = 0, /* FullPrecision: FP32 traversal, FilterStartPoints + copy */
   DK_STRATEGY_HYBRID = 1,         /* Hybrid: PQ traversal, FilterStartPoints + FP32 Rerank  */
   DK_STRATEGY_QUANTIZED = 2,      /* Quantized: PQ traversal, FilterStartPoints + copy      */
+  /* Hybrid-style strategies over low-precision copies of the vectors (no counterpart in the
+   * reference): candidates are scored from BF16 rows, or from FP8-E4M3 rows with one FP32
+   * scale per vector, accumulating in FP32; the queue is then re-ranked with exact FP32
+   * distances (the reference's Rerank, inmem/full_precision.rs:357-404). */
+  DK_STRATEGY_BF16 = 3,
+  DK_STRATEGY_FP8 = 4,
 };
+
+/* dk_index_desc.flags: which low-precision copies dk_index_create derives from `vectors`. */
+#define DK_INDEX_BF16 1u
+#define DK_INDEX_FP8 2u
 
 /* Status codes.  1..4 mirror `KnnSearchError` (diskann/src/graph/search/knn_search.rs:39-44). */
 enum dk_status {
@@ -74,6 +84,7 @@ enum dk_status {
   DK_ERR_ADMISSION = 13,         /* serving loop: request rejected (no slot / memory) */
   DK_ERR_CANCELLED = 14,
   DK_ERR_NOT_FOUND = 15,
+  DK_ERR_NO_LOW_PRECISION = 16,  /* BF16/FP8 strategy on an index created without that copy */
 };
 
 /* Per-query statistics: the reference's `SearchStats` (diskann/src/graph/index.rs:90-102). */
@@ -105,6 +116,7 @@ typedef struct dk_index_desc {
   const float* pq_pivots;     /* 256 x D, row-major */
   const uint8_t* pq_codes;    /* (N+F) rows of `pq_code_stride` bytes, first M used */
   uint64_t pq_code_stride;
+  uint32_t flags;             /* DK_INDEX_BF16 | DK_INDEX_FP8 */
 } dk_index_desc;
 
 typedef struct dk_index dk_index;
