@@ -227,9 +227,9 @@ extern "C" int32_t dk_index_create(const dk_index_desc* d, int32_t device, dk_in
   if (e == cudaSuccess && (d->flags & (DK_INDEX_BF16 | DK_INDEX_FP8)))
     e = dk_build_low_precision(ix, d->flags);
   if (e == cudaSuccess) {
-    e = cudaHostAlloc(reinterpret_cast<void**>(&ix->hint_host), 2 * sizeof(uint32_t), cudaHostAllocMapped);
+    e = cudaHostAlloc(reinterpret_cast<void**>(&ix->hint_host), 8 * sizeof(uint32_t), cudaHostAllocMapped);
     if (e == cudaSuccess) {
-      ix->hint_host[0] = ix->hint_host[1] = 0u;
+      std::memset(ix->hint_host, 0, 8 * sizeof(uint32_t));
       e = cudaHostGetDevicePointer(reinterpret_cast<void**>(&ix->hint_dev), ix->hint_host, 0);
     }
   }

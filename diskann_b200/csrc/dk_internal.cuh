@@ -32,9 +32,10 @@ struct dk_index {
   float* fp8_scale = nullptr;
   uint32_t lp_stride = 0;
   uint64_t bytes = 0;
-  // Visited-set sizing hint in mapped pinned host memory: word 0 = largest
-  // cmps * 256 / (L + F) seen by kernels since the last launch read it, word 1 = the value the
-  // last launch used.  Only performance depends on it (an undersized hash spills, exactly).
+  // Visited-set sizing hint in mapped pinned host memory, in units of cmps * 256 / (L + F):
+  // word 0 = largest value seen by kernels since the last launch read it, 1 = the largest the
+  // last launch used, 2/3 = sum and count of values since the last read, 4 = the mean the
+  // last launch used.  Only performance depends on it (an undersized table spills, exactly).
   uint32_t* hint_host = nullptr;
   uint32_t* hint_dev = nullptr;
 };
@@ -62,6 +63,7 @@ struct SearchParams {
   dk_search_stats* stats;
   // Visited set: shared-memory hash (first pass) or global bitmap slice per CTA (spill pass).
   uint32_t hash_log2;
+  uint32_t hash_slots;  // warp kernel: shared-level slots (any multiple of 32)
   uint32_t hash_limit;  // inserts allowed before the hash counts as full
   uint32_t* bitmap;
   uint32_t bitmap_words;

@@ -113,28 +113,29 @@ struct BitmapSet {
 // the counters are warp-uniform registers updated from ballots.
 struct WarpVisited {
   uint32_t* s;
-  uint32_t smask, sshift, slimit;
+  uint32_t ssize, slimit;  // shared level: any size (multiply-high hashing), at most slimit ids
   uint32_t* g;
   uint32_t gmask, gshift;
   uint32_t scount = 0;  // ids in the shared level
   uint32_t gcount = 0;  // ids in the global level
 
   __device__ void reset(uint32_t lane) {
-    for (uint32_t i = lane; i <= smask; i += 32u) s[i] = kEmpty;
+    for (uint32_t i = lane; i < ssize; i += 32u) s[i] = kEmpty;
     scount = 0u;
     gcount = 0u;
   }
+  __device__ __forceinline__ uint32_t next(uint32_t h) const { return h + 1 == ssize ? 0u : h + 1; }
   // Every lane calls; lanes with `want` test-and-insert their `id`.  True if it was new.
   __device__ bool insert(bool want, uint32_t id) {
     volatile uint32_t* vs = s;
     bool present = false;
-    uint32_t h = (id * 2654435761u) >> sshift;
+    uint32_t h = __umulhi(id * 2654435761u, ssize);
     if (want) {
       while (true) {
         const uint32_t cur = vs[h];
         if (cur == id) { present = true; break; }
         if (cur == kEmpty) break;
-        h = (h + 1) & smask;
+        h = next(h);
       }
     }
     const bool absent = want && !present;
@@ -145,7 +146,7 @@ struct WarpVisited {
     if (absent && rank < room) {
       // Take the first empty slot from the probe's end; other lanes only add other ids.
       while (atomicCAS(&s[h], kEmpty, id) != kEmpty) {
-        do { h = (h + 1) & smask; } while (vs[h] != kEmpty);
+        do { h = next(h); } while (vs[h] != kEmpty);
       }
       fresh = true;
     }
@@ -663,7 +664,12 @@ __device__ __forceinline__ State carve(unsigned char* base, const SearchParams& 
 }
 
 __device__ __forceinline__ void record_hint(const SearchParams& P, uint32_t cmps) {
-  if (P.hint) atomicMax(P.hint, (uint32_t)(((uint64_t)cmps << 8) / P.cap));
+  if (P.hint) {
+    const uint32_t r = (uint32_t)(((uint64_t)cmps << 8) / P.cap);
+    atomicMax(P.hint, r);
+    atomicAdd(P.hint + 2, r);
+    atomicAdd(P.hint + 3, 1u);
+  }
 }
 
 // ========================================================================================
@@ -913,28 +919,108 @@ __global__ void __launch_bounds__(NT) k_search_spill(const SearchParams P) {
 // Warp-per-query kernel.
 // ========================================================================================
 
-// Merge cand_{id,d}[0..count) into the queue; queue bookkeeping lives in registers (the
-// same value in every lane).
-__device__ __forceinline__ void warp_merge(const SearchParams& P, const State& S, uint32_t count,
-                                           uint32_t lane, uint32_t& size, uint32_t& cursor,
-                                           uint32_t& cur) {
+// Order key of a scored candidate at position i: distance ascending (an order-preserving
+// integer image of the float), then position descending (the later insert goes first);
+// NaN and padding sort after every valid key.
+__device__ __forceinline__ uint64_t new_item_key(const float* d, uint32_t i, uint32_t count) {
+  if (i >= count) return ~0ull;
+  const float x = d[i];
+  if (x != x) return ~0ull - 1u;
+  uint32_t u = __float_as_uint(x);
+  u = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+  return ((uint64_t)u << 32) | (uint32_t)~i;
+}
+
+__device__ __forceinline__ uint64_t shfl_xor64(uint64_t v, uint32_t m) {
+  const uint32_t lo = __shfl_xor_sync(kFull, (uint32_t)v, m);
+  const uint32_t hi = __shfl_xor_sync(kFull, (uint32_t)(v >> 32), m);
+  return ((uint64_t)hi << 32) | lo;
+}
+
+// Sort the hop's scored candidates into new_{d,id}[0..nvalid) by (distance ascending,
+// position descending) — the order the reference's one-by-one inserts produce among
+// themselves.  Up to 64 items: a bitonic network over two keys per lane; beyond that a
+// counting rank.  Returns nvalid (NaN distances are dropped).
+__device__ __forceinline__ uint32_t warp_order_new(const State& S, uint32_t count, uint32_t lane) {
   uint32_t nvalid = 0;
-  for (uint32_t i0 = 0; i0 < count; i0 += 32u) {
-    const uint32_t i = i0 + lane;
-    const float d = i < count ? S.cand_d[i] : 0.0f;
-    const bool valid = i < count && d == d;
-    if (valid) {
-      uint32_t r = 0;
-      for (uint32_t j = 0; j < count; ++j) {
-        const float dj = S.cand_d[j];
-        r += (dj < d) || (dj == d && j > i);
+  if (count <= 64u) {
+    uint64_t k0 = new_item_key(S.cand_d, lane, count);
+    uint64_t k1 = new_item_key(S.cand_d, lane + 32u, count);
+    for (uint32_t size = 2; size <= 64u; size <<= 1) {
+      for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+        if (stride == 32u) {  // index lane vs index lane+32, both in this lane; ascending
+          const uint64_t a = min(k0, k1), b = max(k0, k1);
+          k0 = a;
+          k1 = b;
+        } else {
+          const bool lower = (lane & stride) == 0u;
+          const bool asc0 = size == 64u || (lane & size) == 0u;
+          const bool asc1 = size == 64u || ((lane + 32u) & size) == 0u;
+          const uint64_t o0 = shfl_xor64(k0, stride), o1 = shfl_xor64(k1, stride);
+          k0 = (lower == asc0) ? min(k0, o0) : max(k0, o0);
+          k1 = (lower == asc1) ? min(k1, o1) : max(k1, o1);
+        }
       }
-      S.new_d[r] = d;
-      S.new_id[r] = S.cand_id[i];
     }
-    nvalid += __popc(__ballot_sync(kFull, valid));
+    const bool v0 = k0 < ~0ull - 1u, v1 = k1 < ~0ull - 1u;
+    nvalid = __popc(__ballot_sync(kFull, v0)) + __popc(__ballot_sync(kFull, v1));
+    if (v0) {
+      const uint32_t i = ~(uint32_t)k0;
+      S.new_d[lane] = S.cand_d[i];
+      S.new_id[lane] = S.cand_id[i];
+    }
+    if (v1) {
+      const uint32_t i = ~(uint32_t)k1;
+      S.new_d[lane + 32u] = S.cand_d[i];
+      S.new_id[lane + 32u] = S.cand_id[i];
+    }
+  } else {
+    for (uint32_t i0 = 0; i0 < count; i0 += 32u) {
+      const uint32_t i = i0 + lane;
+      const float d = i < count ? S.cand_d[i] : 0.0f;
+      const bool valid = i < count && d == d;
+      if (valid) {
+        uint32_t r = 0;
+        for (uint32_t j = 0; j < count; ++j) {
+          const float dj = S.cand_d[j];
+          r += (dj < d) || (dj == d && j > i);
+        }
+        S.new_d[r] = d;
+        S.new_id[r] = S.cand_id[i];
+      }
+      nvalid += __popc(__ballot_sync(kFull, valid));
+    }
   }
   __syncwarp();
+  return nvalid;
+}
+
+// Position of the first unvisited entry after merging the ordered new items (the next node
+// to expand) and that node's id, or kEmpty when the queue will hold no unvisited entry.
+__device__ __forceinline__ uint32_t warp_next_cursor(const SearchParams& P, const State& S,
+                                                     uint32_t nvalid, uint32_t size,
+                                                     uint32_t cursor, uint32_t cur,
+                                                     uint32_t& next_id) {
+  const uint32_t new_size = min(size + nvalid, P.cap);
+  const float* od = S.qd[cur];
+  uint32_t nc = new_size;
+  next_id = kEmpty;
+  if (cursor < size) {
+    const uint32_t p = cursor + count_less_equal(S.new_d, nvalid, od[cursor]);
+    if (p < nc) { nc = p; next_id = S.qi[cur][cursor] & kIdMask; }
+  }
+  if (nvalid > 0) {
+    const uint32_t p = count_less(od, size, S.new_d[0]);
+    if (p < nc) { nc = p; next_id = S.new_id[0]; }
+  }
+  return nc;
+}
+
+// Write the merged queue into the other buffer (see the file comment for the order rule).
+__device__ __forceinline__ void warp_commit_merge(const SearchParams& P, const State& S,
+                                                  uint32_t nvalid, uint32_t nc, uint32_t lane,
+                                                  uint32_t& size, uint32_t& cursor,
+                                                  uint32_t& cur) {
   const uint32_t cap = P.cap, nxt = cur ^ 1u;
   const uint32_t new_size = min(size + nvalid, cap);
   const float* od = S.qd[cur];
@@ -951,13 +1037,19 @@ __device__ __forceinline__ void warp_merge(const SearchParams& P, const State& S
     const uint32_t pos = r + count_less(od, size, d);
     if (pos < cap) { wd[pos] = d; wi[pos] = S.new_id[r]; }
   }
-  uint32_t nc = new_size;
-  if (cursor < size) nc = min(nc, cursor + count_less_equal(S.new_d, nvalid, od[cursor]));
-  if (nvalid > 0) nc = min(nc, count_less(od, size, S.new_d[0]));
   cursor = nc;
   size = new_size;
   cur = nxt;
   __syncwarp();
+}
+
+__device__ __forceinline__ void warp_merge(const SearchParams& P, const State& S, uint32_t count,
+                                           uint32_t lane, uint32_t& size, uint32_t& cursor,
+                                           uint32_t& cur) {
+  const uint32_t nvalid = warp_order_new(S, count, lane);
+  uint32_t next_id;
+  const uint32_t nc = warp_next_cursor(P, S, nvalid, size, cursor, cur, next_id);
+  warp_commit_merge(P, S, nvalid, nc, lane, size, cursor, cur);
 }
 
 template <int METRIC, int MODE, int DIM, int U>
@@ -1056,6 +1148,9 @@ __device__ __forceinline__ void warp_query(const SearchParams& P, const State& S
   warp_merge(P, S, P.f, lane, size, cursor, cur);
   uint32_t cmps = P.f, hops = 0;
   uint32_t* beam = S.misc->beam;
+  // Adjacency row of the next node, fetched while the previous hop's merge runs (beam 1:
+  // the next node is known as soon as the hop's candidates are scored).
+  uint32_t pf_node = kEmpty, pf_deg = 0, pf_ids[4] = {0u, 0u, 0u, 0u};
 
   while (cursor < size) {
     // closest_notvisited x beam (queue.rs:297-313); `cursor` is the first unvisited entry.
@@ -1091,13 +1186,21 @@ __device__ __forceinline__ void warp_query(const SearchParams& P, const State& S
     // Expand: adjacency rows in beam order, ids through the visited set in order.
     uint32_t count = 0;
     for (uint32_t b = 0; b < nb; ++b) {
-      const uint32_t* row = P.adj + (size_t)beam[b] * P.astride;
-      const uint32_t deg = __ldg(row);
+      const uint32_t node = beam[b];
+      const uint32_t* row = P.adj + (size_t)node * P.astride;
+      uint32_t deg;
       uint32_t ids[4];
+      if (b == 0 && node == pf_node) {
+        deg = pf_deg;
 #pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        const uint32_t t = 32u * r + lane;
-        ids[r] = t < P.max_degree ? __ldg(row + 1 + t) : 0u;
+        for (int r = 0; r < 4; ++r) ids[r] = pf_ids[r];
+      } else {
+        deg = __ldg(row);
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const uint32_t t = 32u * r + lane;
+          ids[r] = t < P.max_degree ? __ldg(row + 1 + t) : 0u;
+        }
       }
       for (uint32_t t0 = 0; t0 < deg; t0 += 32u) {
         const uint32_t t = t0 + lane;
@@ -1116,7 +1219,20 @@ __device__ __forceinline__ void warp_query(const SearchParams& P, const State& S
     }
     __syncwarp();
     warp_score<METRIC, MODE, DIM, U>(P, S, S.cand_id, S.cand_d, count, lane);
-    warp_merge(P, S, count, lane, size, cursor, cur);
+    const uint32_t nvalid = warp_order_new(S, count, lane);
+    uint32_t next_id;
+    const uint32_t nc = warp_next_cursor(P, S, nvalid, size, cursor, cur, next_id);
+    pf_node = P.beam == 1 ? next_id : kEmpty;
+    if (pf_node != kEmpty) {
+      const uint32_t* row = P.adj + (size_t)pf_node * P.astride;
+      pf_deg = __ldg(row);
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const uint32_t t = 32u * r + lane;
+        pf_ids[r] = t < P.max_degree ? __ldg(row + 1 + t) : 0u;
+      }
+    }
+    warp_commit_merge(P, S, nvalid, nc, lane, size, cursor, cur);
     cmps += count;
     hops += nb;
   }
@@ -1138,8 +1254,7 @@ __global__ void __launch_bounds__(128) k_search_warp(const SearchParams P) {
   const State S = carve(smem + (size_t)warp * P.warp_smem, P);
   WarpVisited vset;
   vset.s = S.hash;
-  vset.smask = (1u << P.hash_log2) - 1u;
-  vset.sshift = 32u - P.hash_log2;
+  vset.ssize = P.hash_slots;
   vset.slimit = P.hash_limit;
   vset.g = P.gtable + ((size_t)slot << P.gtable_log2);
   vset.gmask = (1u << P.gtable_log2) - 1u;

@@ -114,6 +114,7 @@ int32_t dk_launch_search(const dk_index* ix, int32_t strategy, const float* quer
   // 1.1 * max_degree * 1.3 * L).  Only performance depends on these sizes: a query whose
   // visited set outgrows them re-runs exactly in the bitmap spill pass.
   double ratio = 0.5 * 1.1 * 1.3 * ix->max_degree;
+  double mean_ratio = ratio;
   P.hint = ix->hint_dev;
   if (ix->hint_host) {
     volatile uint32_t* h = ix->hint_host;
@@ -122,9 +123,17 @@ int32_t dk_launch_search(const dk_index* ix, int32_t strategy, const float* quer
       h[1] = seen;
       h[0] = 0;
     }
+    const uint32_t sum = h[2], cnt = h[3];
+    if (cnt) {
+      h[4] = (uint32_t)((sum + cnt - 1) / cnt);
+      h[2] = 0;
+      h[3] = 0;
+    }
     if (h[1]) ratio = (double)h[1] / 256.0 * 1.15;
+    if (h[4]) mean_ratio = (double)h[4] / 256.0;
   }
   const double est = ratio * (double)P.cap + beam * ix->max_degree + ix->f;
+  const double est_mean = mean_ratio * (double)P.cap + beam * ix->max_degree + ix->f;
 
   int dev = 0, max_optin = 0, sms = 0;
   cudaGetDevice(&dev);
@@ -143,18 +152,22 @@ int32_t dk_launch_search(const dk_index* ix, int32_t strategy, const float* quer
   uint64_t gtable_bytes = 0;
   cudaError_t e = cudaSuccess;
   if (warp) {
-    // Small shared level sized to a per-warp shared-memory budget (many queries per SM);
-    // the global level holds the rest of the learned visited-set size.
+    // Shared level: room for 1.3x the mean visited set at <= 3/4 load, within a per-warp
+    // shared-memory budget; the global level takes what a longer search adds.
     L.kind = dk::KernelKind::kWarp;
     P.hash_log2 = 0;
     const uint32_t base = plan_query_smem(P, pq, false);
-    const uint32_t budget = std::max<uint32_t>(env_u32("DK_WARP_SMEM", 8192), base + 1024);
-    uint32_t hl = 8;
-    while (hl < 16 && base + (4u << (hl + 1)) <= budget) ++hl;
-    P.hash_log2 = env_u32("DK_HASH_LOG2", hl);
-    P.hash_log2 = std::min<uint32_t>(std::max<uint32_t>(P.hash_log2, 6), 16);
-    P.hash_limit = (uint32_t)((1u << P.hash_log2) * 0.75);
-    P.warp_smem = plan_query_smem(P, pq, true);
+    const uint32_t budget = std::max<uint32_t>(env_u32("DK_WARP_SMEM", 24576), base + 1024);
+    uint32_t slots = align_up((uint32_t)(est_mean * 1.3 / 0.75) + 1, 32);
+    slots = std::min<uint32_t>(slots, ((budget - base) / 4) & ~31u);
+    if (const uint32_t hl = env_u32("DK_HASH_LOG2", 0)) slots = 1u << std::min<uint32_t>(hl, 16);
+    slots = std::max<uint32_t>(slots, 64);
+    P.hash_slots = slots;
+    P.hash_limit = slots * 3 / 4;
+    P.hash_log2 = log2_at_least(slots, 6, 16);  // only sizes the shared-memory carve-up below
+    P.warp_smem = base + align_up(slots * 4, 16);
+    plan_query_smem(P, pq, false);
+    P.off_hash = base;
     if (P.warp_smem > (uint32_t)max_optin) return too_big();
     P.gtable_log2 = log2_at_least(std::max(est, 2.0 * P.hash_limit) / 0.75, 10, 22);
     P.gtable_log2 = std::min<uint32_t>(std::max<uint32_t>(env_u32("DK_GTABLE_LOG2", P.gtable_log2), 6), 24);

