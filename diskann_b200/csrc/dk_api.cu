@@ -45,7 +45,8 @@ void free_index(dk_index* ix) {
   cudaFree(ix->vec_bf16);
   cudaFree(ix->vec_fp8);
   cudaFree(ix->fp8_scale);
-  if (ix->hint_host) cudaFreeHost(ix->hint_host);
+  cudaFree(ix->hint_dev);
+  if (ix->hint_stage) cudaFreeHost(ix->hint_stage);
   cudaSetDevice(prev);
   delete ix;
 }
@@ -227,11 +228,11 @@ extern "C" int32_t dk_index_create(const dk_index_desc* d, int32_t device, dk_in
   if (e == cudaSuccess && (d->flags & (DK_INDEX_BF16 | DK_INDEX_FP8)))
     e = dk_build_low_precision(ix, d->flags);
   if (e == cudaSuccess) {
-    e = cudaHostAlloc(reinterpret_cast<void**>(&ix->hint_host), 8 * sizeof(uint32_t), cudaHostAllocMapped);
-    if (e == cudaSuccess) {
-      std::memset(ix->hint_host, 0, 8 * sizeof(uint32_t));
-      e = cudaHostGetDevicePointer(reinterpret_cast<void**>(&ix->hint_dev), ix->hint_host, 0);
-    }
+    e = cudaMalloc(reinterpret_cast<void**>(&ix->hint_dev), 4 * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMemset(ix->hint_dev, 0, 4 * sizeof(uint32_t));
+    if (e == cudaSuccess)
+      e = cudaHostAlloc(reinterpret_cast<void**>(&ix->hint_stage), 4 * sizeof(uint32_t), cudaHostAllocDefault);
+    if (e == cudaSuccess) std::memset(ix->hint_stage, 0, 4 * sizeof(uint32_t));
   }
   if (e != cudaSuccess) {
     free_index(ix);

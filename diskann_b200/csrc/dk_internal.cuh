@@ -32,12 +32,15 @@ struct dk_index {
   float* fp8_scale = nullptr;
   uint32_t lp_stride = 0;
   uint64_t bytes = 0;
-  // Visited-set sizing hint in mapped pinned host memory, in units of cmps * 256 / (L + F):
-  // word 0 = largest value seen by kernels since the last launch read it, 1 = the largest the
-  // last launch used, 2/3 = sum and count of values since the last read, 4 = the mean the
-  // last launch used.  Only performance depends on it (an undersized table spills, exactly).
-  uint32_t* hint_host = nullptr;
+  // Visited-set sizing hint, in units of cmps * 256 / (L + F).  Kernels update three device
+  // words (largest value, sum, count) with L2 atomics; each launch sequence ends with an
+  // asynchronous copy of them to pinned host memory (`hint_stage`) and a reset, and the next
+  // launch plans from the staged values.  Only performance depends on the hint: an
+  // undersized visited table spills, exactly.
   uint32_t* hint_dev = nullptr;
+  uint32_t* hint_stage = nullptr;
+  uint32_t hint_max = 0;   // last staged largest value
+  uint32_t hint_mean = 0;  // last staged mean
 };
 
 // Per-launch parameters of the beam-search kernels.
@@ -115,7 +118,7 @@ cudaError_t dk_build_low_precision(dk_index* ix, uint32_t flags);
 
 // Launch the search (first pass + spill pass) on `stream`.  Parameters are validated by
 // the caller.
-int32_t dk_launch_search(const dk_index* ix, int32_t strategy, const float* queries,
+int32_t dk_launch_search(dk_index* ix, int32_t strategy, const float* queries,
                          uint64_t qstride, uint32_t nq, uint32_t k, uint32_t l, uint32_t beam,
                          uint32_t* ids, float* dists, dk_search_stats* stats,
                          cudaStream_t stream);

@@ -663,12 +663,12 @@ __device__ __forceinline__ State carve(unsigned char* base, const SearchParams& 
   return S;
 }
 
-__device__ __forceinline__ void record_hint(const SearchParams& P, uint32_t cmps) {
-  if (P.hint) {
-    const uint32_t r = (uint32_t)(((uint64_t)cmps << 8) / P.cap);
+__device__ __forceinline__ void record_hint(const SearchParams& P, uint32_t cmps, uint32_t cap) {
+  if (P.hint) {  // device memory: L2 atomics
+    const uint32_t r = (uint32_t)(((uint64_t)cmps << 8) / cap);
     atomicMax(P.hint, r);
-    atomicAdd(P.hint + 2, r);
-    atomicAdd(P.hint + 3, 1u);
+    atomicAdd(P.hint + 1, r);
+    atomicAdd(P.hint + 2, 1u);
   }
 }
 
@@ -890,7 +890,7 @@ __global__ void __launch_bounds__(NT) k_search_cta(const SearchParams P) {
   __syncthreads();
   if (threadIdx.x == 0) {
     P.stats[qid] = dk_search_stats{cmps, hops, S.misc->result_count, 0u};
-    record_hint(P, cmps);
+    record_hint(P, cmps, P.cap);
   }
 }
 
@@ -909,7 +909,7 @@ __global__ void __launch_bounds__(NT) k_search_spill(const SearchParams P) {
     __syncthreads();
     if (threadIdx.x == 0) {
       P.stats[qid] = dk_search_stats{cmps, hops, S.misc->result_count, kFlagSpilled};
-      record_hint(P, cmps);
+      record_hint(P, cmps, P.cap);
     }
     __syncthreads();
   }
@@ -997,11 +997,11 @@ __device__ __forceinline__ uint32_t warp_order_new(const State& S, uint32_t coun
 
 // Position of the first unvisited entry after merging the ordered new items (the next node
 // to expand) and that node's id, or kEmpty when the queue will hold no unvisited entry.
-__device__ __forceinline__ uint32_t warp_next_cursor(const SearchParams& P, const State& S,
+__device__ __forceinline__ uint32_t warp_next_cursor(uint32_t cap, const State& S,
                                                      uint32_t nvalid, uint32_t size,
                                                      uint32_t cursor, uint32_t cur,
                                                      uint32_t& next_id) {
-  const uint32_t new_size = min(size + nvalid, P.cap);
+  const uint32_t new_size = min(size + nvalid, cap);
   const float* od = S.qd[cur];
   uint32_t nc = new_size;
   next_id = kEmpty;
@@ -1017,11 +1017,11 @@ __device__ __forceinline__ uint32_t warp_next_cursor(const SearchParams& P, cons
 }
 
 // Write the merged queue into the other buffer (see the file comment for the order rule).
-__device__ __forceinline__ void warp_commit_merge(const SearchParams& P, const State& S,
+__device__ __forceinline__ void warp_commit_merge(uint32_t cap, const State& S,
                                                   uint32_t nvalid, uint32_t nc, uint32_t lane,
                                                   uint32_t& size, uint32_t& cursor,
                                                   uint32_t& cur) {
-  const uint32_t cap = P.cap, nxt = cur ^ 1u;
+  const uint32_t nxt = cur ^ 1u;
   const uint32_t new_size = min(size + nvalid, cap);
   const float* od = S.qd[cur];
   const uint32_t* oi = S.qi[cur];
@@ -1043,14 +1043,24 @@ __device__ __forceinline__ void warp_commit_merge(const SearchParams& P, const S
   __syncwarp();
 }
 
-__device__ __forceinline__ void warp_merge(const SearchParams& P, const State& S, uint32_t count,
+__device__ __forceinline__ void warp_merge(uint32_t cap, const State& S, uint32_t count,
                                            uint32_t lane, uint32_t& size, uint32_t& cursor,
                                            uint32_t& cur) {
   const uint32_t nvalid = warp_order_new(S, count, lane);
   uint32_t next_id;
-  const uint32_t nc = warp_next_cursor(P, S, nvalid, size, cursor, cur, next_id);
-  warp_commit_merge(P, S, nvalid, nc, lane, size, cursor, cur);
+  const uint32_t nc = warp_next_cursor(cap, S, nvalid, size, cursor, cur, next_id);
+  warp_commit_merge(cap, S, nvalid, nc, lane, size, cursor, cur);
 }
+
+// One query's inputs and outputs (a batch row, or a serving request).
+struct QueryIO {
+  const float* query;
+  uint32_t k;
+  uint32_t cap;  // L + F
+  uint32_t* ids;
+  float* dists;
+  dk_search_stats* stats;
+};
 
 template <int METRIC, int MODE, int DIM, int U>
 __device__ __forceinline__ void warp_score(const SearchParams& P, const State& S,
@@ -1070,17 +1080,18 @@ __device__ __forceinline__ void warp_score(const SearchParams& P, const State& S
 }
 
 template <int METRIC, int DIM, int U>
-__device__ void warp_post_process(const SearchParams& P, const State& S, uint32_t qid,
+__device__ void warp_post_process(const SearchParams& P, const State& S, const QueryIO& io,
                                   uint32_t lane, uint32_t size, uint32_t cur,
                                   uint32_t& result_count) {
   const float* qd = S.qd[cur];
   const uint32_t* qi = S.qi[cur];
-  uint32_t* out_ids = P.out_ids + (size_t)qid * P.k;
-  float* out_d = P.out_dists + (size_t)qid * P.k;
+  uint32_t* out_ids = io.ids;
+  float* out_d = io.dists;
+  const uint32_t k = io.k;
   const bool hybrid = strategy_reranks(P.strategy);
   uint32_t base = 0;
   for (uint32_t t0 = 0; t0 < size; t0 += 32u) {
-    if (!hybrid && base >= P.k) break;
+    if (!hybrid && base >= k) break;
     const uint32_t i = t0 + lane;
     const uint32_t id = i < size ? (qi[i] & kIdMask) : 0u;
     const bool keep = i < size && id < P.n;  // FilterStartPoints (glue.rs:730-773)
@@ -1088,13 +1099,13 @@ __device__ void warp_post_process(const SearchParams& P, const State& S, uint32_
     const uint32_t pos = base + __popc(m & lanemask_lt());
     if (keep) {
       if (hybrid) S.cand_id[pos] = id;
-      else if (pos < P.k) { out_ids[pos] = id; out_d[pos] = qd[i]; }
+      else if (pos < k) { out_ids[pos] = id; out_d[pos] = qd[i]; }
     }
     base += __popc(m);
   }
   uint32_t written;
   if (!hybrid) {
-    written = min(base, P.k);
+    written = min(base, k);
   } else {
     // Rerank (inmem/full_precision.rs:357-404): exact distances, stable sort, first k.
     const uint32_t count = base;
@@ -1104,16 +1115,16 @@ __device__ void warp_post_process(const SearchParams& P, const State& S, uint32_
       const float d = S.cand_d[i];
       const bool dn = d != d;
       uint32_t r = 0;
-      for (uint32_t j = 0; j < count && r < P.k; ++j) {
+      for (uint32_t j = 0; j < count && r < k; ++j) {
         const float dj = S.cand_d[j];
         const bool jn = dj != dj;
         r += dn ? (jn && j < i) : (!jn && (dj < d || (dj == d && j < i)));
       }
-      if (r < P.k) { out_ids[r] = S.cand_id[i]; out_d[r] = d; }
+      if (r < k) { out_ids[r] = S.cand_id[i]; out_d[r] = d; }
     }
-    written = min(count, P.k);
+    written = min(count, k);
   }
-  for (uint32_t j = written + lane; j < P.k; j += 32u) {
+  for (uint32_t j = written + lane; j < k; j += 32u) {
     out_ids[j] = DK_INVALID_ID;
     out_d[j] = INFINITY;
   }
@@ -1123,8 +1134,9 @@ __device__ void warp_post_process(const SearchParams& P, const State& S, uint32_
 // One query, run by one warp.  Writes the query's outputs and stats (or the spill flag).
 template <int METRIC, int MODE, int DIM, int U>
 __device__ __forceinline__ void warp_query(const SearchParams& P, const State& S,
-                                           WarpVisited& vset, uint32_t qid, uint32_t lane) {
-  const float* qsrc = P.queries + (size_t)qid * P.qstride;
+                                           WarpVisited& vset, const QueryIO& io, uint32_t lane) {
+  const float* qsrc = io.query;
+  const uint32_t cap = io.cap;
   const uint32_t dpad = (P.dim + 15u) & ~15u;  // zero padded: FP8 pieces hold 16 elements
   for (uint32_t i = lane; i < dpad; i += 32u) S.q[i] = i < P.dim ? qsrc[i] : 0.0f;
   vset.reset(lane);
@@ -1134,7 +1146,7 @@ __device__ __forceinline__ void warp_query(const SearchParams& P, const State& S
     __syncwarp();
   }
   if (P.f + P.beam * P.max_degree > P.gtable_limit) {
-    if (lane == 0) P.stats[qid] = dk_search_stats{0u, 0u, 0u, kFlagSpilled};
+    if (lane == 0) *io.stats = dk_search_stats{0u, 0u, 0u, kFlagSpilled};
     return;
   }
   uint32_t size = 0, cursor = 0, cur = 0;
@@ -1145,7 +1157,7 @@ __device__ __forceinline__ void warp_query(const SearchParams& P, const State& S
   }
   __syncwarp();
   warp_score<METRIC, MODE, DIM, U>(P, S, S.cand_id, S.cand_d, P.f, lane);
-  warp_merge(P, S, P.f, lane, size, cursor, cur);
+  warp_merge(cap, S, P.f, lane, size, cursor, cur);
   uint32_t cmps = P.f, hops = 0;
   uint32_t* beam = S.misc->beam;
   // Adjacency row of the next node, fetched while the previous hop's merge runs (beam 1:
@@ -1180,7 +1192,7 @@ __device__ __forceinline__ void warp_query(const SearchParams& P, const State& S
     __syncwarp();
     // The global level must keep room for a whole hop going there; otherwise spill.
     if (vset.gcount + nb * P.max_degree > P.gtable_limit) {
-      if (lane == 0) P.stats[qid] = dk_search_stats{0u, 0u, 0u, kFlagSpilled};
+      if (lane == 0) *io.stats = dk_search_stats{0u, 0u, 0u, kFlagSpilled};
       return;
     }
     // Expand: adjacency rows in beam order, ids through the visited set in order.
@@ -1221,7 +1233,7 @@ __device__ __forceinline__ void warp_query(const SearchParams& P, const State& S
     warp_score<METRIC, MODE, DIM, U>(P, S, S.cand_id, S.cand_d, count, lane);
     const uint32_t nvalid = warp_order_new(S, count, lane);
     uint32_t next_id;
-    const uint32_t nc = warp_next_cursor(P, S, nvalid, size, cursor, cur, next_id);
+    const uint32_t nc = warp_next_cursor(cap, S, nvalid, size, cursor, cur, next_id);
     pf_node = P.beam == 1 ? next_id : kEmpty;
     if (pf_node != kEmpty) {
       const uint32_t* row = P.adj + (size_t)pf_node * P.astride;
@@ -1232,15 +1244,15 @@ __device__ __forceinline__ void warp_query(const SearchParams& P, const State& S
         pf_ids[r] = t < P.max_degree ? __ldg(row + 1 + t) : 0u;
       }
     }
-    warp_commit_merge(P, S, nvalid, nc, lane, size, cursor, cur);
+    warp_commit_merge(cap, S, nvalid, nc, lane, size, cursor, cur);
     cmps += count;
     hops += nb;
   }
   uint32_t result_count = 0;
-  warp_post_process<METRIC, DIM, U>(P, S, qid, lane, size, cur, result_count);
+  warp_post_process<METRIC, DIM, U>(P, S, io, lane, size, cur, result_count);
   if (lane == 0) {
-    P.stats[qid] = dk_search_stats{cmps, hops, result_count, 0u};
-    record_hint(P, cmps);
+    *io.stats = dk_search_stats{cmps, hops, result_count, 0u};
+    record_hint(P, cmps, cap);
   }
 }
 
@@ -1269,7 +1281,10 @@ __global__ void __launch_bounds__(128) k_search_warp(const SearchParams P) {
       for (uint32_t i = lane; i <= vset.gmask; i += 32u) vset.g[i] = kEmpty;
       __syncwarp();
     }
-    warp_query<METRIC, MODE, DIM, U>(P, S, vset, qid, lane);
+    const QueryIO io{P.queries + (size_t)qid * P.qstride, P.k, P.cap,
+                     P.out_ids + (size_t)qid * P.k, P.out_dists + (size_t)qid * P.k,
+                     P.stats + qid};
+    warp_query<METRIC, MODE, DIM, U>(P, S, vset, io, lane);
     __syncwarp();
     gdirty = vset.gcount != 0u;
   }

@@ -68,7 +68,7 @@ int32_t too_big() {
 
 }  // namespace
 
-int32_t dk_launch_search(const dk_index* ix, int32_t strategy, const float* queries,
+int32_t dk_launch_search(dk_index* ix, int32_t strategy, const float* queries,
                          uint64_t qstride, uint32_t nq, uint32_t k, uint32_t l, uint32_t beam,
                          uint32_t* ids, float* dists, dk_search_stats* stats,
                          cudaStream_t stream) {
@@ -108,29 +108,21 @@ int32_t dk_launch_search(const dk_index* ix, int32_t strategy, const float* quer
   P.list_cap = std::max(std::max(beam * ix->max_degree, P.cap), ix->f);
 
   // Visited-set size.  |visited| equals the comparison count, which for a given graph grows
-  // about linearly with L + F.  The largest ratio is learned from previous launches on this
-  // index (kernels record cmps / (L + F) in mapped host memory); before any launch the
-  // prior is half the reference's own upper-bound estimate (scratch.rs:186-193,
-  // 1.1 * max_degree * 1.3 * L).  Only performance depends on these sizes: a query whose
-  // visited set outgrows them re-runs exactly in the bitmap spill pass.
+  // about linearly with L + F.  The largest and the mean ratio are learned from previous
+  // launches on this index (see dk_index::hint_dev); before any launch the prior is half the
+  // reference's own upper-bound estimate (scratch.rs:186-193, 1.1 * max_degree * 1.3 * L).
+  // Only performance depends on these sizes: a query whose visited set outgrows them
+  // re-runs exactly in the bitmap spill pass.
   double ratio = 0.5 * 1.1 * 1.3 * ix->max_degree;
   double mean_ratio = ratio;
   P.hint = ix->hint_dev;
-  if (ix->hint_host) {
-    volatile uint32_t* h = ix->hint_host;
-    const uint32_t seen = h[0];
-    if (seen) {
-      h[1] = seen;
-      h[0] = 0;
-    }
-    const uint32_t sum = h[2], cnt = h[3];
-    if (cnt) {
-      h[4] = (uint32_t)((sum + cnt - 1) / cnt);
-      h[2] = 0;
-      h[3] = 0;
-    }
-    if (h[1]) ratio = (double)h[1] / 256.0 * 1.15;
-    if (h[4]) mean_ratio = (double)h[4] / 256.0;
+  {
+    volatile uint32_t* h = ix->hint_stage;  // written by the previous launch's async copy
+    const uint32_t seen = h[0], sum = h[1], cnt = h[2];
+    if (seen) ix->hint_max = seen;
+    if (cnt) ix->hint_mean = (uint32_t)(((uint64_t)sum + cnt - 1) / cnt);
+    if (ix->hint_max) ratio = (double)ix->hint_max / 256.0 * 1.15;
+    if (ix->hint_mean) mean_ratio = (double)ix->hint_mean / 256.0;
   }
   const double est = ratio * (double)P.cap + beam * ix->max_degree + ix->f;
   const double est_mean = mean_ratio * (double)P.cap + beam * ix->max_degree + ix->f;
@@ -241,6 +233,10 @@ int32_t dk_launch_search(const dk_index* ix, int32_t strategy, const float* quer
   L.spill_ctas = spill_ctas;
   if (e == cudaSuccess) e = dispatch(ix->metric, L, mode, stream);
   cudaFreeAsync(scratch, stream);
+  // Stage this launch's visited-size statistics for the next launch's planning, then reset.
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(ix->hint_stage, ix->hint_dev, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(ix->hint_dev, 0, 3 * sizeof(uint32_t), stream);
   if (e != cudaSuccess) {
     dk_set_error(DK_ERR_CUDA, std::string("search launch: ") + cudaGetErrorString(e));
     return DK_ERR_CUDA;

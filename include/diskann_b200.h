@@ -85,6 +85,7 @@ enum dk_status {
   DK_ERR_CANCELLED = 14,
   DK_ERR_NOT_FOUND = 15,
   DK_ERR_NO_LOW_PRECISION = 16,  /* BF16/FP8 strategy on an index created without that copy */
+  DK_ERR_NOT_READY = 17,         /* serving: the request has not completed yet */
 };
 
 /* Per-query statistics: the reference's `SearchStats` (diskann/src/graph/index.rs:90-102). */
@@ -159,6 +160,45 @@ int32_t dk_search_device(dk_index* index, int32_t strategy, const float* queries
                          uint32_t beam_width, uint32_t* ids, float* dists,
                          dk_search_stats* stats, void* stream);
 
+
+/* ---- Serving: a persistent device loop with continuous admission (no counterpart in the
+ * reference, whose searches are one call per query on host tasks) ----
+ *
+ * dk_server_create starts a device loop whose warps each own one search slot (shared-memory
+ * beam state and a visited set sized for max_l).  dk_server_submit copies one request into a
+ * ring in pinned host memory and publishes it; a free slot on the device claims it while
+ * other requests are in flight, so requests of different k and L overlap on the GPU.
+ * dk_server_poll returns DK_OK once the request's results are in the caller's buffers, or
+ * DK_ERR_NOT_READY.  Admission: a submit is rejected with DK_ERR_ADMISSION when
+ * queue_depth requests are outstanding; slots are sized from shared memory and device
+ * memory at creation.  Every device-side wait is bounded: the loop exits after idle_ms
+ * without work (the next submit or poll restarts it) and when the server is destroyed. */
+typedef struct dk_server dk_server;
+
+typedef struct dk_server_config {
+  int32_t strategy;      /* enum dk_strategy, for every request */
+  uint32_t max_k;        /* per-request k <= max_k */
+  uint32_t max_l;        /* per-request L <= max_l */
+  uint32_t beam_width;   /* for every request */
+  uint32_t queue_depth;  /* outstanding requests accepted (ring size) */
+  uint32_t max_slots;    /* device slots (0 = as many as fit) */
+  uint32_t idle_ms;      /* device loop exits after this long without work (0 = 200) */
+} dk_server_config;
+
+typedef struct dk_server_info {
+  uint32_t slots;            /* concurrent searches on the device */
+  uint32_t queue_depth;
+  uint64_t device_bytes;     /* HBM held by the server (visited-set tables, ring state) */
+  uint64_t launches;         /* device-loop launches so far */
+} dk_server_info;
+
+int32_t dk_server_create(dk_index* index, const dk_server_config* config, dk_server** out);
+int32_t dk_server_submit(dk_server* server, const float* query, uint32_t k, uint32_t l,
+                         uint64_t* ticket);
+int32_t dk_server_poll(dk_server* server, uint64_t ticket, uint32_t* ids, float* dists,
+                       dk_search_stats* stats);
+int32_t dk_server_get_info(const dk_server* server, dk_server_info* info);
+int32_t dk_server_destroy(dk_server* server);
 
 /* ---- Data tooling on either side of the search path (host code, no GPU needed) ---- */
 
