@@ -36,15 +36,15 @@ sys.path.insert(0, ROOT)
 WORKLOADS = {
     "pq1m": dict(n=1_000_000, dim=128, comps=256, sigma=8.0, nq=10_000, R=64, l_build=100,
                  alpha=1.2, pq_chunks=32, pq_train=100_000, k=10,
-                 l_sweep=[50, 75, 100, 150, 200, 250, 300, 400], strategy="hybrid",
-                 seed=0xD15CA77 + 1),
+                 l_sweep=[50, 75, 100, 150, 200, 250, 300, 400],
+                 strategies=["fp32", "bf16", "fp8", "hybrid"], seed=0xD15CA77 + 1),
     "fp100k": dict(n=100_000, dim=128, comps=64, sigma=10.0, nq=1000, R=32, l_build=50,
-                   alpha=1.2, pq_chunks=0, pq_train=0, k=10, l_sweep=[100], strategy="full",
-                   seed=0xD15CA77),
+                   alpha=1.2, pq_chunks=0, pq_train=0, k=10, l_sweep=[50, 75, 100, 150, 200],
+                   strategies=["fp32", "bf16", "fp8"], seed=0xD15CA77),
     "pq100k": dict(n=100_000, dim=128, comps=256, sigma=8.0, nq=10_000, R=64, l_build=100,
                    alpha=1.2, pq_chunks=32, pq_train=100_000, k=10,
-                   l_sweep=[50, 75, 100, 150, 200, 250, 300, 400], strategy="hybrid",
-                   seed=0xD15CA77 + 11),
+                   l_sweep=[50, 75, 100, 150, 200, 250, 300, 400],
+                   strategies=["fp32", "bf16", "fp8", "hybrid"], seed=0xD15CA77 + 11),
 }
 TARGET_RECALL = 0.95
 METRIC_NAME = "QPS at recall@10>=0.95"
@@ -166,27 +166,90 @@ class ClockSampler:
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
 
 
+STRATEGY_CODES = ("fp32", "bf16", "fp8", "hybrid")
+DTYPE_OF = {"fp32": "f32", "bf16": "bf16 (f32 accumulate, exact f32 rerank)",
+            "fp8": "fp8-e4m3 (per-vector f32 scale, f32 accumulate, exact f32 rerank)",
+            "hybrid": "u8 PQ codes (f32 ADC table, exact f32 rerank)"}
+
+
+def strategy_objects():
+    from diskann_b200 import BF16, FP8, FullPrecision, Hybrid
+
+    return {"fp32": FullPrecision(), "bf16": BF16(), "fp8": FP8(), "hybrid": Hybrid()}
+
+
 def algorithmic_bytes(stats, w, l, mean_degree, strategy):
     """Bytes one batch must move (per query, summed): one adjacency row per expanded node
-    (length word + ids), one scored item per comparison (a PQ code or a full vector), the
-    full vectors of the rerank, the query; plus the PQ pivot table once per batch."""
+    (length word + ids), one scored item per comparison (a full f32 row, a BF16 or FP8 row
+    (+ its f32 scale), or a PQ code), the f32 rows of the exact rerank (at most L), the query;
+    plus the PQ pivot table once per batch."""
     hops = stats["hops"].astype(np.float64)
     cmps = stats["cmps"].astype(np.float64)
     d = w["dim"]
+    lp = (d + 15) // 16 * 16
     per = hops * (4 + 4 * mean_degree) + d * 4
-    if strategy == "full":
+    extra = 0.0
+    if strategy == "fp32":
         per = per + cmps * d * 4
-        extra = 0.0
+    elif strategy == "bf16":
+        per = per + cmps * lp * 2 + l * d * 4
+    elif strategy == "fp8":
+        per = per + cmps * (lp + 4) + l * d * 4
     else:
-        per = per + cmps * w["pq_chunks"] + (l if strategy == "hybrid" else 0) * d * 4
+        per = per + cmps * w["pq_chunks"] + l * d * 4
         extra = 256.0 * d * 4
     return float(per.sum() + extra)
+
+
+def stats_array(st):
+    out = np.zeros(st.shape[0], dtype=[("cmps", np.uint32), ("hops", np.uint32),
+                                       ("result_count", np.uint32), ("flags", np.uint32)])
+    for i, f in enumerate(("cmps", "hops", "result_count", "flags")):
+        out[f] = st[:, i]
+    return out
+
+
+def serve_latency(provider, strategy, queries, k, l, rate, seconds, seed=1):
+    """Poisson arrivals at `rate` requests/s through the serving API (dk_server_*); latency is
+    completion seen by the host minus scheduled arrival.  Returns p50/p99 (ms) and the rate
+    achieved."""
+    from diskann_b200 import SearchServer
+
+    srv = SearchServer(provider, strategy, max_k=k, max_l=l, queue_depth=8192)
+    nq = queries.shape[0]
+    srv.wait(srv.submit(queries[0], k, l), k)
+    n = max(1, int(rate * seconds))
+    arrivals = np.cumsum(np.random.default_rng(seed).exponential(1.0 / rate, size=n))
+    lat = np.zeros(n)
+    outstanding = {}
+    i = done = 0
+    t0 = time.perf_counter()
+    while done < n:
+        now = time.perf_counter() - t0
+        while i < n and arrivals[i] <= now:
+            outstanding[srv.submit(queries[i % nq], k, l)] = i
+            i += 1
+        for t in list(outstanding):
+            if srv.poll(t, k) is not None:
+                j = outstanding.pop(t)
+                lat[j] = time.perf_counter() - t0 - arrivals[j]
+                done += 1
+        if time.perf_counter() - t0 > seconds * 4 + 10:
+            break
+    elapsed = time.perf_counter() - t0
+    info = srv.info()
+    srv.close()
+    lat = np.sort(lat[:done])
+    pick = lambda p: float(lat[min(int(p * len(lat) / 100), len(lat) - 1)]) * 1e3
+    return {"offered_qps": rate, "achieved_qps": round(done / elapsed, 1), "requests": done,
+            "p50_ms": round(pick(50), 4), "p99_ms": round(pick(99), 4),
+            "launches": int(info["launches"]), "streams": int(info["streams"])}
 
 
 def run_ours(args, data, rank, world):
     import torch
 
-    from diskann_b200 import DiskANNIndex, FullPrecision, GpuProvider, Hybrid, Knn, Metric, Quantized
+    from diskann_b200 import DiskANNIndex, GpuProvider, Knn, Metric
     from diskann_b200.groundtruth import recall_at_k
 
     w = data["w"]
@@ -194,10 +257,10 @@ def run_ours(args, data, rank, world):
     torch.cuda.set_device(dev)
     t0 = time.time()
     provider = GpuProvider(data["vectors"], data["adj"], data["deg"], data["n"], Metric.L2,
-                           pq=data["pq"], device=dev)
+                           pq=data["pq"], device=dev, low_precision=("bf16", "fp8"))
     idx = DiskANNIndex(provider)
     log(f"[ours] index upload {time.time() - t0:.1f}s, {provider.info()['device_bytes'] / 2**20:.0f} MiB")
-    strategy = {"hybrid": Hybrid(), "full": FullPrecision(), "quantized": Quantized()}[w["strategy"]]
+    strategies = strategy_objects()
     queries = data["queries"]
     nq, k = queries.shape[0], w["k"]
     gt = data["gt"]
@@ -206,43 +269,47 @@ def run_ours(args, data, rank, world):
     dists = torch.empty((nq, k), dtype=torch.float32, device=dq.device)
     stats = torch.empty((nq, 4), dtype=torch.int32, device=dq.device)
     stream = torch.cuda.current_stream(dq.device)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dq.device)  # 256 MiB > 126 MB L2
 
     def search(params, strat):
         idx.search_device(params, strat, dq, ids, dists, stats, stream)
 
-    # Recall sweep: smallest L reaching the target.
-    chosen = None
-    sweep = {}
-    for l in w["l_sweep"]:
-        search(Knn(k, l), strategy)
-        torch.cuda.synchronize()
-        r = recall_at_k(ids.cpu().numpy().view(np.uint32), gt, k)
-        sweep[l] = round(r, 4)
-        if chosen is None and r >= TARGET_RECALL:
-            chosen = l
-    if chosen is None:
-        chosen = w["l_sweep"][-1]
-    log(f"[ours] recall sweep {sweep} -> L={chosen}")
-    params = Knn(k, chosen)
+    def timed(params, strat, reps=3):
+        ts = []
+        for _ in range(reps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            search(params, strat)
+            b.record(stream)
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b))
+        return nq / (float(np.median(ts)) / 1e3)
 
-    # Plain FP32 path at the same target, for the BF16/PQ-vs-FP32 comparison.
-    fp32 = None
-    if w["strategy"] != "full":
-        for l in [l for l in (50, 75, 100, 150, 200, 300) if l >= k]:
-            search(Knn(k, l), FullPrecision())
+    # Per strategy: the smallest L of the sweep whose recall@10 reaches the target, timed.
+    table = {}
+    for name in w["strategies"]:
+        if name == "hybrid" and data["pq"] is None:
+            continue
+        strat = strategies[name]
+        row = None
+        for l in w["l_sweep"]:
+            search(Knn(k, l), strat)
             torch.cuda.synchronize()
             r = recall_at_k(ids.cpu().numpy().view(np.uint32), gt, k)
+            row = {"L": l, "recall": round(r, 4), "reached": r >= TARGET_RECALL}
             if r >= TARGET_RECALL:
-                s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                search(Knn(k, l), FullPrecision())
-                s0.record(stream)
-                search(Knn(k, l), FullPrecision())
-                s1.record(stream)
-                torch.cuda.synchronize()
-                fp32 = {"L": l, "recall": round(r, 4), "qps": nq / (s0.elapsed_time(s1) / 1e3)}
                 break
-
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dq.device)  # 256 MiB > 126 MB L2
+        row["qps"] = round(timed(Knn(k, row["L"]), strat), 1)
+        table[name] = row
+        log(f"[ours] {name}: {row}")
+    reached = {n: r for n, r in table.items() if r["reached"]}
+    pool = reached or table
+    head = max(pool, key=lambda n: pool[n]["qps"])
+    chosen = table[head]["L"]
+    strategy = strategies[head]
+    params = Knn(k, chosen)
+    log(f"[ours] headline strategy {head} at L={chosen}")
 
     for _ in range(args.warmup):
         flush.zero_()
@@ -262,11 +329,7 @@ def run_ours(args, data, rank, world):
     barrier(world)
     elapsed_ms = sum(a.elapsed_time(b) for a, b in ev)
     elapsed_ms = max_over_ranks(elapsed_ms, world)
-    st = stats.cpu().numpy().view(np.uint32)
-    stats_np = np.zeros(nq, dtype=[("cmps", np.uint32), ("hops", np.uint32),
-                                   ("result_count", np.uint32), ("flags", np.uint32)])
-    for i, f in enumerate(("cmps", "hops", "result_count", "flags")):
-        stats_np[f] = st[:, i]
+    stats_np = stats_array(stats.cpu().numpy().view(np.uint32))
     rec = recall_at_k(ids.cpu().numpy().view(np.uint32), gt, k)
     ms_per_step = elapsed_ms / args.steps
     value = world * nq / (ms_per_step / 1e3)
@@ -283,23 +346,53 @@ def run_ours(args, data, rank, world):
         if s >= args.warmup:
             e2e_t.append(t1 - t0)
     e2e_s = max_over_ranks(float(np.mean(e2e_t)) * 1e3, world) / 1e3
+
+    # Serving: Poisson arrivals through dk_server_* at two offered rates (rank 0 of N=1 only).
+    serving = None
+    if world == 1 and not args.no_serving:
+        serving = [serve_latency(provider, strategy, queries, k, chosen, rate, args.serve_seconds)
+                   for rate in (2000.0, 20000.0)]
+        log(f"[ours] serving {serving}")
+
     mean_deg = float(data["deg"][: data["n"]].mean())
-    alg = algorithmic_bytes(stats_np, w, chosen, mean_deg, w["strategy"])
+    alg = algorithmic_bytes(stats_np, w, chosen, mean_deg, head)
     achieved = alg / (ms_per_step / 1e3) / 1e9
     peak, peak_src = hbm_peak()
-    cl = clocks.summary()
-    return dict(value=value, ms_per_step=ms_per_step, recall=rec, L=chosen, sweep=sweep, fp32=fp32,
+    fp32_row = table.get("fp32")
+    fp32_alg = None
+    if fp32_row is not None:
+        search(Knn(k, fp32_row["L"]), strategies["fp32"])
+        torch.cuda.synchronize()
+        st32 = stats_array(stats.cpu().numpy().view(np.uint32))
+        fp32_alg = algorithmic_bytes(st32, w, fp32_row["L"], mean_deg, "fp32")
+        fp32_row = dict(fp32_row, roofline_frac=round(
+            fp32_alg * fp32_row["qps"] / nq / 1e9 / peak, 4))
+    return dict(value=value, ms_per_step=ms_per_step, recall=rec, L=chosen, strategy=head,
+                strategies=table, fp32=fp32_row, serving=serving,
                 e2e=dict(value=world * nq / e2e_s, unit="queries/s",
                          h2d_bytes_per_step=int(queries.nbytes),
                          d2h_bytes_per_step=int(nq * k * 8 + nq * 16)),
                 roofline=dict(bound="hbm", achieved=round(achieved, 1), peak=peak, unit="GB/s",
-                              frac=round(achieved / peak, 4), traffic=None,
+                              frac=round(achieved / peak, 4),
+                              traffic=traffic_from_profile(head, nq),
                               algorithmic_bytes_per_step=int(alg), peak_source=peak_src),
-                clocks=cl,
+                clocks=clocks.summary(),
                 stats=dict(cmps_mean=float(stats_np["cmps"].mean()),
                            hops_mean=float(stats_np["hops"].mean()),
                            spilled=int((stats_np["flags"] & 1).sum())),
                 gpu_launches=2 * args.steps)
+
+
+def traffic_from_profile(strategy, nq):
+    """DRAM bytes (read + write) per launch of the headline kernel, from the committed ncu
+    summary of the same workload (scaled to `nq` queries), or None."""
+    p = os.path.join(ROOT, "profiles", "dram_traffic_pq1m.json")
+    try:
+        with open(p) as f:
+            rec = json.load(f)[strategy]
+        return int(rec["dram_bytes"] * nq / rec["queries"])
+    except Exception:
+        return None
 
 
 def hbm_peak():
@@ -311,21 +404,29 @@ def hbm_peak():
         return 6650.0, "fallback"
 
 
-def cpu_baseline(data, l, threads, min_seconds=2.0, max_reps=5):
-    """Oracle (CPU restatement of the reference search) on all host threads."""
+def oracle_strategy(name):
     from oracle import oracle as orc
 
-    w = data["w"]
+    return {"hybrid": orc.STRATEGY_HYBRID, "fp32": orc.STRATEGY_FULL_PRECISION}[name]
+
+
+def oracle_index(data):
+    from oracle import oracle as orc
+
     pq = data["pq"]
-    o = orc.OracleIndex(data["vectors"], data["adj"], data["deg"], data["n"], orc.METRIC_L2,
-                        *(tuple() if pq is None else (pq.offsets, pq.pivots, pq.codes)))
-    strat = {"hybrid": orc.STRATEGY_HYBRID, "full": orc.STRATEGY_FULL_PRECISION,
-             "quantized": orc.STRATEGY_QUANTIZED}[w["strategy"]]
-    q = data["queries"]
+    return orc.OracleIndex(data["vectors"], data["adj"], data["deg"], data["n"], orc.METRIC_L2,
+                           *(tuple() if pq is None else (pq.offsets, pq.pivots, pq.codes)))
+
+
+def cpu_baseline(data, strategy, l, threads, min_seconds=2.0, max_reps=5, nq=None):
+    """Oracle (CPU restatement of the reference search) on `threads` host threads."""
+    w = data["w"]
+    o = oracle_index(data)
+    q = data["queries"] if nq is None else data["queries"][:nq]
     total, reps, t0 = 0, 0, time.perf_counter()
     res = None
     while reps < max_reps and (time.perf_counter() - t0 < min_seconds or reps == 0):
-        res = o.search(q, w["k"], l, 1, strat, threads=threads)
+        res = o.search(q, w["k"], l, 1, oracle_strategy(strategy), threads=threads)
         total += q.shape[0]
         reps += 1
     el = time.perf_counter() - t0
@@ -350,32 +451,28 @@ def max_over_ranks(x: float, world: int) -> float:
     return float(t.item())
 
 
-def choose_l_on_cpu(data):
+def choose_l_on_cpu(data, strategy):
     """Smallest L of the sweep whose oracle recall reaches the target (same rule as ours)."""
     from diskann_b200.groundtruth import recall_at_k
-    from oracle import oracle as orc
 
     w = data["w"]
-    pq = data["pq"]
-    o = orc.OracleIndex(data["vectors"], data["adj"], data["deg"], data["n"], orc.METRIC_L2,
-                        *(tuple() if pq is None else (pq.offsets, pq.pivots, pq.codes)))
-    strat = {"hybrid": orc.STRATEGY_HYBRID, "full": orc.STRATEGY_FULL_PRECISION,
-             "quantized": orc.STRATEGY_QUANTIZED}[w["strategy"]]
+    o = oracle_index(data)
     for l in w["l_sweep"]:
-        ids, _, _ = o.search(data["queries"], w["k"], l, 1, strat, threads=os.cpu_count() or 1)
+        ids, _, _ = o.search(data["queries"], w["k"], l, 1, oracle_strategy(strategy),
+                             threads=os.cpu_count() or 1)
         if recall_at_k(ids, data["gt"], w["k"]) >= TARGET_RECALL:
             return l
     return w["l_sweep"][-1]
 
 
-def config_of(w, name, l):
+def config_of(w, name, l, strategy):
     return {
         "workload": (f"{name}: {w['n']:,} x {w['dim']} f32 Gaussian mixture ({w['comps']} comp, "
                      f"sigma {w['sigma']}), Vamana R={w['R']} L_build={w['l_build']} "
                      f"alpha={w['alpha']}" + (f", PQ {w['pq_chunks']}x256" if w["pq_chunks"] else "")
-                     + f", {w['nq']:,} queries, k={w['k']}, L={l}, strategy={w['strategy']}"),
+                     + f", {w['nq']:,} queries, k={w['k']}, L={l}, strategy={strategy}"),
         "n_points": w["n"], "dim": w["dim"], "queries_per_step": w["nq"], "k": w["k"], "L": l,
-        "strategy": w["strategy"], "metric": "L2", "l2_flush": "256 MiB write before every step",
+        "strategy": strategy, "metric": "L2", "l2_flush": "256 MiB write before every step",
         "parallelism": "replicas",
     }
 
@@ -389,6 +486,8 @@ def main():
     ap.add_argument("--workload", default="pq1m", choices=sorted(WORKLOADS))
     ap.add_argument("--cache", default=os.environ.get("DK_BENCH_CACHE", "/tmp/diskann_b200_bench"))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--serve-seconds", type=float, default=2.0)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -397,27 +496,33 @@ def main():
     threads = os.cpu_count() or 1
 
     if args.impl == "reference":
+        # The reference's search on the host cores: the oracle port (the reference is Rust and
+        # no Rust toolchain is available to build it), plain FP32 search at the smallest L of
+        # the sweep reaching the recall target, all host threads.  Each step is a bounded
+        # sample of the query batch.
         if rank != 0:
             return 0
         data = prepare(args.workload, 0, args.cache)
         w = data["w"]
-        l = choose_l_on_cpu(data)
+        l = choose_l_on_cpu(data, "fp32")
+        sample = min(w["nq"], 4000)
         times = []
         for s in range(args.warmup + args.steps):
-            t0 = time.perf_counter()
-            qps, _, _ = cpu_baseline(data, l, threads, min_seconds=0.0, max_reps=1)
+            qps, _, _ = cpu_baseline(data, "fp32", l, threads, min_seconds=0.0, max_reps=1,
+                                     nq=sample)
             if s >= args.warmup:
-                times.append(w["nq"] / qps)
+                times.append(sample / qps)
         ms = float(np.mean(times)) * 1e3
-        value = w["nq"] / (ms / 1e3)
+        value = sample / (ms / 1e3)
         line = {"impl": "reference", "metric": METRIC_NAME, "value": round(value, 1),
                 "unit": "queries/s", "n_gpus": args.gpus, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": config_of(w, args.workload, l),
+                "config": config_of(w, args.workload, l, "fp32"),
                 "cpu_baseline": {"value": round(value, 1), "unit": "queries/s", "cores": threads,
                                  "kind": "port",
-                                 "sample": f"all {w['nq']} queries per step, {threads} threads"},
+                                 "sample": f"{sample} of the {w['nq']} queries per step, "
+                                           f"{threads} threads, FullPrecision L={l}"},
                 "e2e": {"value": round(value, 1), "unit": "queries/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
@@ -437,17 +542,24 @@ def main():
     if rank == 0:
         cpu = None
         if not args.no_cpu_baseline and world == 1:
-            qps, reps, _ = cpu_baseline(data, r["L"], threads)
+            cpu_strat = r["strategy"] if r["strategy"] in ("fp32", "hybrid") else "fp32"
+            cpu_l = r["L"] if cpu_strat == r["strategy"] else (r["fp32"] or {}).get("L", r["L"])
+            sample = min(w["nq"], 4000)
+            qps, reps, _ = cpu_baseline(data, cpu_strat, cpu_l, threads, nq=sample)
             cpu = {"value": round(qps, 1), "unit": "queries/s", "cores": threads, "kind": "port",
-                   "sample": f"{reps} x {w['nq']} queries, {threads} threads, L={r['L']}"}
+                   "sample": f"{reps} x {sample} queries, {threads} threads, "
+                             f"{cpu_strat} L={cpu_l}"}
         line = {
             "metric": METRIC_NAME, "value": round(r["value"], 1), "unit": "queries/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(r["ms_per_step"], 4), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": config_of(w, args.workload, r["L"]),
-            "recall_at_10": round(r["recall"], 4), "recall_sweep": r["sweep"],
+            "vs_baseline": None, "dtype": DTYPE_OF[r["strategy"]], "data": "synthetic",
+            "config": config_of(w, args.workload, r["L"], r["strategy"]),
+            "recall_at_10": round(r["recall"], 4), "strategies": r["strategies"],
             "fp32_path_at_target": r["fp32"],
+            "vs_fp32_path": (round(r["value"] / world / r["fp32"]["qps"], 3)
+                             if r["fp32"] else None),
+            "serving": r["serving"],
             "e2e": {k: (round(v, 1) if isinstance(v, float) else v) for k, v in r["e2e"].items()},
             "gpu_launches": r["gpu_launches"], "roofline": r["roofline"], "cpu_baseline": cpu,
             "clocks": r["clocks"], "search_stats": r["stats"],

@@ -20,10 +20,11 @@ from .index import (  # noqa: F401
     PQData,
     Quantized,
     STATS_DTYPE,
+    SearchServer,
     Status,
 )
 
 __all__ = [
     "ANNError", "BF16", "DiskANNIndex", "FP8", "FullPrecision", "GpuProvider", "Hybrid", "Knn",
-    "KnnSearchError", "Metric", "PQData", "Quantized", "STATS_DTYPE", "Status",
+    "KnnSearchError", "Metric", "PQData", "Quantized", "STATS_DTYPE", "SearchServer", "Status",
 ]

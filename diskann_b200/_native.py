@@ -24,6 +24,11 @@ EXPORTED_SYMBOLS = (
     "dk_index_get_info",
     "dk_search",
     "dk_search_device",
+    "dk_server_create",
+    "dk_server_submit",
+    "dk_server_poll",
+    "dk_server_get_info",
+    "dk_server_destroy",
     "dk_distance",
     "dk_compute_medoid",
     "dk_build_vamana",
@@ -70,6 +75,29 @@ class IndexInfo(ctypes.Structure):
     ]
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [
+        ("strategy", ctypes.c_int32),
+        ("max_k", ctypes.c_uint32),
+        ("max_l", ctypes.c_uint32),
+        ("beam_width", ctypes.c_uint32),
+        ("queue_depth", ctypes.c_uint32),
+        ("max_slots", ctypes.c_uint32),
+        ("streams", ctypes.c_uint32),
+    ]
+
+
+class ServerInfo(ctypes.Structure):
+    _fields_ = [
+        ("slots", ctypes.c_uint32),
+        ("queue_depth", ctypes.c_uint32),
+        ("streams", ctypes.c_uint32),
+        ("pad", ctypes.c_uint32),
+        ("device_bytes", ctypes.c_uint64),
+        ("launches", ctypes.c_uint64),
+    ]
+
+
 _lock = threading.Lock()
 _lib = None
 
@@ -103,6 +131,16 @@ def load():
         L.dk_search.argtypes = [vp, i32, vp, u64, u32, u32, u32, u32, vp, vp, vp]
         L.dk_search_device.restype = i32
         L.dk_search_device.argtypes = [vp, i32, vp, u64, u32, u32, u32, u32, vp, vp, vp, vp]
+        L.dk_server_create.restype = i32
+        L.dk_server_create.argtypes = [vp, ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]
+        L.dk_server_submit.restype = i32
+        L.dk_server_submit.argtypes = [vp, vp, u32, u32, ctypes.POINTER(u64)]
+        L.dk_server_poll.restype = i32
+        L.dk_server_poll.argtypes = [vp, u64, vp, vp, vp]
+        L.dk_server_get_info.restype = i32
+        L.dk_server_get_info.argtypes = [vp, ctypes.POINTER(ServerInfo)]
+        L.dk_server_destroy.restype = i32
+        L.dk_server_destroy.argtypes = [vp]
         _lib = L
         return L
 

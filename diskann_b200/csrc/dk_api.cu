@@ -47,6 +47,7 @@ void free_index(dk_index* ix) {
   cudaFree(ix->fp8_scale);
   cudaFree(ix->hint_dev);
   if (ix->hint_stage) cudaFreeHost(ix->hint_stage);
+  if (ix->pool) cudaMemPoolDestroy(ix->pool);
   cudaSetDevice(prev);
   delete ix;
 }
@@ -65,8 +66,11 @@ struct DeviceGuard {
   }
 };
 
-int32_t check_search_args(const dk_index* ix, int32_t strategy, uint32_t k, uint32_t l,
-                          uint32_t beam, uint64_t qstride) {
+
+}  // namespace
+
+int32_t dk_check_search_args(const dk_index* ix, int32_t strategy, uint32_t k, uint32_t l,
+                             uint32_t beam, uint64_t qstride) {
   if (!ix) return fail(DK_ERR_INVALID_ARGUMENT, "index is null");
   const int32_t v = dk_knn_validate(k, l, beam);
   if (v != DK_OK) return v;
@@ -86,8 +90,6 @@ int32_t check_search_args(const dk_index* ix, int32_t strategy, uint32_t k, uint
   if (qstride < ix->dim) return fail(DK_ERR_DIMENSION_MISMATCH, "query stride below dim");
   return DK_OK;
 }
-
-}  // namespace
 
 void dk_set_error(int32_t status, const std::string& msg) {
   g_last_status = status;
@@ -234,6 +236,15 @@ extern "C" int32_t dk_index_create(const dk_index_desc* d, int32_t device, dk_in
       e = cudaHostAlloc(reinterpret_cast<void**>(&ix->hint_stage), 4 * sizeof(uint32_t), cudaHostAllocDefault);
     if (e == cudaSuccess) std::memset(ix->hint_stage, 0, 4 * sizeof(uint32_t));
   }
+  if (e == cudaSuccess) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    e = cudaMemPoolCreate(&ix->pool, &props);
+    uint64_t keep = UINT64_MAX;
+    if (e == cudaSuccess) e = cudaMemPoolSetAttribute(ix->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
   if (e != cudaSuccess) {
     free_index(ix);
     return cuda_fail(e, "index upload");
@@ -265,7 +276,7 @@ extern "C" int32_t dk_search_device(dk_index* ix, int32_t strategy, const float*
                                     uint64_t query_stride, uint32_t nq, uint32_t k, uint32_t l,
                                     uint32_t beam_width, uint32_t* ids, float* dists,
                                     dk_search_stats* stats, void* stream) {
-  const int32_t v = check_search_args(ix, strategy, k, l, beam_width, query_stride);
+  const int32_t v = dk_check_search_args(ix, strategy, k, l, beam_width, query_stride);
   if (v != DK_OK) return v;
   if (nq && (!queries || !ids || !dists || !stats))
     return fail(DK_ERR_INVALID_ARGUMENT, "queries, ids, dists and stats are required");
@@ -278,7 +289,7 @@ extern "C" int32_t dk_search(dk_index* ix, int32_t strategy, const float* querie
                              uint64_t query_stride, uint32_t nq, uint32_t k, uint32_t l,
                              uint32_t beam_width, uint32_t* ids, float* dists,
                              dk_search_stats* stats) {
-  const int32_t v = check_search_args(ix, strategy, k, l, beam_width, query_stride);
+  const int32_t v = dk_check_search_args(ix, strategy, k, l, beam_width, query_stride);
   if (v != DK_OK) return v;
   if (nq == 0) return DK_OK;
   if (!queries || !ids || !dists) return fail(DK_ERR_INVALID_ARGUMENT, "queries, ids and dists are required");
@@ -294,10 +305,10 @@ extern "C" int32_t dk_search(dk_index* ix, int32_t strategy, const float* querie
   const size_t off_st = off_d + round_up(obytes * 4, 256);
   const size_t total = off_st + (size_t)nq * sizeof(dk_search_stats);
   int32_t rc = DK_OK;
-  e = cudaMallocAsync(reinterpret_cast<void**>(&buf), total, s);
+  e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&buf), total, ix->pool, s);
   if (e != cudaSuccess) {
     cudaStreamDestroy(s);
-    return cuda_fail(e, "cudaMallocAsync");
+    return cuda_fail(e, "cudaMallocFromPoolAsync");
   }
   float* dq = reinterpret_cast<float*>(buf);
   uint32_t* dids = reinterpret_cast<uint32_t*>(buf + off_ids);

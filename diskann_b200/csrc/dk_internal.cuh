@@ -41,6 +41,10 @@ struct dk_index {
   uint32_t* hint_stage = nullptr;
   uint32_t hint_max = 0;   // last staged largest value
   uint32_t hint_mean = 0;  // last staged mean
+  // Stream-ordered scratch of every search on this index comes from this pool, which keeps
+  // freed memory reserved (release threshold: unlimited), so a repeated search reuses it
+  // instead of mapping new memory each call.
+  cudaMemPool_t pool = nullptr;
 };
 
 // Per-launch parameters of the beam-search kernels.
@@ -83,7 +87,10 @@ struct SearchParams {
   uint32_t smem_bytes;
   uint32_t warp_smem;
   uint32_t list_cap;  // capacity of the candidate / rerank lists
-  uint32_t* hint;     // device view of dk_index::hint_host (may be null)
+  uint32_t* hint;     // device words of the visited-size hint (may be null)
+  // Serving launches: per-request (k, L) pairs; outputs keep a stride of `k` (= max_k).
+  // Null for batch launches, where every query uses `k` and `l`.
+  const uint32_t* req_kl;
 };
 
 constexpr uint32_t kFlagSpilled = 1u;
@@ -112,6 +119,10 @@ __host__ __device__ inline bool strategy_reranks(int32_t strategy) {
 
 // Thread-local error reporting for the C ABI.
 void dk_set_error(int32_t status, const std::string& msg);
+
+// Argument checks shared by every search entry point (sets the thread's error).
+int32_t dk_check_search_args(const dk_index* ix, int32_t strategy, uint32_t k, uint32_t l,
+                             uint32_t beam, uint64_t qstride);
 
 // Derive the low-precision copies requested by `flags` from the index's FP32 rows.
 cudaError_t dk_build_low_precision(dk_index* ix, uint32_t flags);

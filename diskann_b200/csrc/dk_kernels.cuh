@@ -1281,7 +1281,9 @@ __global__ void __launch_bounds__(128) k_search_warp(const SearchParams P) {
       for (uint32_t i = lane; i <= vset.gmask; i += 32u) vset.g[i] = kEmpty;
       __syncwarp();
     }
-    const QueryIO io{P.queries + (size_t)qid * P.qstride, P.k, P.cap,
+    const uint32_t qk = P.req_kl ? P.req_kl[2 * qid] : P.k;
+    const uint32_t qcap = P.req_kl ? P.req_kl[2 * qid + 1] + P.f : P.cap;
+    const QueryIO io{P.queries + (size_t)qid * P.qstride, qk, qcap,
                      P.out_ids + (size_t)qid * P.k, P.out_dists + (size_t)qid * P.k,
                      P.stats + qid};
     warp_query<METRIC, MODE, DIM, U>(P, S, vset, io, lane);
@@ -1305,6 +1307,7 @@ struct LaunchPlan {
   uint32_t spill_ctas;
   uint32_t score_u;    // warp kernel, D <= 128: rows per subgroup per round (2 or 4)
   bool query_only;     // warp kernel: only report `blocks_per_sm` for `warps_per_cta`
+  bool skip_spill;     // serving launches: spilled requests are re-run by the host
   int blocks_per_sm;
 };
 
@@ -1329,7 +1332,7 @@ cudaError_t launch_variant(LaunchPlan& L, cudaStream_t stream) {
     if (DIM > 0 && DIM <= 128 && L.score_u >= 4) e = launch_warp<METRIC, MODE, DIM, 4>(L, stream);
     else if (DIM > 0 && DIM <= 128) e = launch_warp<METRIC, MODE, DIM, 2>(L, stream);
     else e = launch_warp<METRIC, MODE, DIM, 1>(L, stream);
-    if (e != cudaSuccess || L.query_only) return e;
+    if (e != cudaSuccess || L.query_only || L.skip_spill) return e;
   } else {
     auto k1 = k_search_cta<kCtaThreads, METRIC, MODE, DIM>;
     e = cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.p1.smem_bytes);
@@ -1365,6 +1368,20 @@ cudaError_t dk_launch_cosine(dk::LaunchPlan& L, int mode, cudaStream_t stream);
 cudaError_t dk_launch_cosine_normalized(dk::LaunchPlan& L, int mode, cudaStream_t stream);
 
 namespace dk {
+// Host planning shared by the batch path and the serving path (dk_search.cu).
+// Lay out one query's shared-memory state in `P`; returns its size in bytes.
+uint32_t plan_query_smem(SearchParams& P, bool pq, bool with_hash);
+// Fill the index and list fields of `P` for k, L (capacity L + F) and the beam width.
+void base_params(const dk_index* ix, int32_t strategy, uint32_t k, uint32_t l, uint32_t beam,
+                 SearchParams& P);
+// Visited-set size estimates (largest, mean) for the queue capacity in `P`.
+void visited_estimates(dk_index* ix, const SearchParams& P, double& est, double& est_mean);
+// Plan a warp-per-query launch (shared level, global level, warps per CTA, and a grid of at
+// most `max_warps` warps, capped at the resident maximum); returns a dk_status.
+int32_t plan_warp(dk_index* ix, SearchParams& P, LaunchPlan& L, int mode, double est,
+                  double est_mean, uint64_t max_warps, cudaStream_t stream);
+cudaError_t dispatch(int32_t metric, LaunchPlan& L, int mode, cudaStream_t stream);
+
 // All scoring modes of one metric (PQ traversal is not offered with the Cosine metric).
 template <int METRIC>
 cudaError_t launch_modes(LaunchPlan& L, int mode, cudaStream_t stream) {

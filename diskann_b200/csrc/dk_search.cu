@@ -17,7 +17,27 @@ namespace {
 inline uint32_t align_up(uint32_t x, uint32_t a) { return (x + a - 1) / a * a; }
 inline uint64_t align_up64(uint64_t x, uint64_t a) { return (x + a - 1) / a * a; }
 
-// Lay out one query's shared-memory state; returns its size in bytes.
+uint32_t env_u32(const char* name, uint32_t dflt) {
+  const char* v = getenv(name);
+  if (!v || !*v) return dflt;
+  return (uint32_t)strtoul(v, nullptr, 10);
+}
+
+uint32_t log2_at_least(double x, uint32_t lo, uint32_t hi) {
+  uint32_t l = lo;
+  while (l < hi && (double)(1u << l) < x) ++l;
+  return l;
+}
+
+int32_t too_big() {
+  dk_set_error(DK_ERR_UNSUPPORTED, "search state does not fit in shared memory (L or PQ too large)");
+  return DK_ERR_UNSUPPORTED;
+}
+
+}  // namespace
+
+namespace dk {
+
 uint32_t plan_query_smem(SearchParams& P, bool pq, bool with_hash) {
   uint32_t off = 0;
   auto take = [&](uint32_t bytes) {
@@ -40,19 +60,7 @@ uint32_t plan_query_smem(SearchParams& P, bool pq, bool with_hash) {
   return off;
 }
 
-uint32_t env_u32(const char* name, uint32_t dflt) {
-  const char* v = getenv(name);
-  if (!v || !*v) return dflt;
-  return (uint32_t)strtoul(v, nullptr, 10);
-}
-
-uint32_t log2_at_least(double x, uint32_t lo, uint32_t hi) {
-  uint32_t l = lo;
-  while (l < hi && (double)(1u << l) < x) ++l;
-  return l;
-}
-
-cudaError_t dispatch(int32_t metric, dk::LaunchPlan& L, int mode, cudaStream_t stream) {
+cudaError_t dispatch(int32_t metric, LaunchPlan& L, int mode, cudaStream_t stream) {
   switch (metric) {
     case DK_METRIC_L2: return dk_launch_l2(L, mode, stream);
     case DK_METRIC_INNER_PRODUCT: return dk_launch_ip(L, mode, stream);
@@ -61,21 +69,8 @@ cudaError_t dispatch(int32_t metric, dk::LaunchPlan& L, int mode, cudaStream_t s
   }
 }
 
-int32_t too_big() {
-  dk_set_error(DK_ERR_UNSUPPORTED, "search state does not fit in shared memory (L or PQ too large)");
-  return DK_ERR_UNSUPPORTED;
-}
-
-}  // namespace
-
-int32_t dk_launch_search(dk_index* ix, int32_t strategy, const float* queries,
-                         uint64_t qstride, uint32_t nq, uint32_t k, uint32_t l, uint32_t beam,
-                         uint32_t* ids, float* dists, dk_search_stats* stats,
-                         cudaStream_t stream) {
-  if (nq == 0) return DK_OK;
-  const int mode = mode_of_strategy(strategy);
-  const bool pq = mode == kModePQ;
-  SearchParams P{};
+void base_params(const dk_index* ix, int32_t strategy, uint32_t k, uint32_t l, uint32_t beam,
+                 SearchParams& P) {
   P.vectors = ix->vectors;
   P.adj = ix->adj;
   P.codes = ix->codes;
@@ -94,28 +89,23 @@ int32_t dk_launch_search(dk_index* ix, int32_t strategy, const float* queries,
   P.max_degree = ix->max_degree;
   P.cstride = ix->cstride;
   P.pq_chunks = ix->pq_chunks;
-  P.queries = queries;
-  P.qstride = qstride;
-  P.nq = nq;
   P.k = k;
   P.l = l;
   P.cap = l + ix->f;
   P.beam = beam;
   P.strategy = strategy;
-  P.out_ids = ids;
-  P.out_dists = dists;
-  P.stats = stats;
   P.list_cap = std::max(std::max(beam * ix->max_degree, P.cap), ix->f);
+}
 
-  // Visited-set size.  |visited| equals the comparison count, which for a given graph grows
-  // about linearly with L + F.  The largest and the mean ratio are learned from previous
-  // launches on this index (see dk_index::hint_dev); before any launch the prior is half the
-  // reference's own upper-bound estimate (scratch.rs:186-193, 1.1 * max_degree * 1.3 * L).
-  // Only performance depends on these sizes: a query whose visited set outgrows them
-  // re-runs exactly in the bitmap spill pass.
+void visited_estimates(dk_index* ix, const SearchParams& P, double& est, double& est_mean) {
+  // |visited| equals the comparison count, which for a given graph grows about linearly with
+  // L + F.  The largest and the mean ratio are learned from previous launches on this index
+  // (see dk_index::hint_dev); before any launch the prior is half the reference's own
+  // upper-bound estimate (scratch.rs:186-193, 1.1 * max_degree * 1.3 * L).  Only performance
+  // depends on these sizes: a query whose visited set outgrows them re-runs exactly in the
+  // bitmap spill pass.
   double ratio = 0.5 * 1.1 * 1.3 * ix->max_degree;
   double mean_ratio = ratio;
-  P.hint = ix->hint_dev;
   {
     volatile uint32_t* h = ix->hint_stage;  // written by the previous launch's async copy
     const uint32_t seen = h[0], sum = h[1], cnt = h[2];
@@ -124,8 +114,83 @@ int32_t dk_launch_search(dk_index* ix, int32_t strategy, const float* queries,
     if (ix->hint_max) ratio = (double)ix->hint_max / 256.0 * 1.15;
     if (ix->hint_mean) mean_ratio = (double)ix->hint_mean / 256.0;
   }
-  const double est = ratio * (double)P.cap + beam * ix->max_degree + ix->f;
-  const double est_mean = mean_ratio * (double)P.cap + beam * ix->max_degree + ix->f;
+  est = ratio * (double)P.cap + P.beam * ix->max_degree + ix->f;
+  est_mean = mean_ratio * (double)P.cap + P.beam * ix->max_degree + ix->f;
+}
+
+int32_t plan_warp(dk_index* ix, SearchParams& P, LaunchPlan& L, int mode, double est,
+                  double est_mean, uint64_t max_warps, cudaStream_t stream) {
+  const bool pq = mode == kModePQ;
+  int dev = 0, max_optin = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  // Shared level: room for 1.3x the mean visited set at <= 3/4 load, within a per-warp
+  // shared-memory budget; the global level takes what a longer search adds.
+  P.hash_log2 = 0;
+  const uint32_t base = plan_query_smem(P, pq, false);
+  const uint32_t budget = std::max<uint32_t>(env_u32("DK_WARP_SMEM", 24576), base + 1024);
+  uint32_t slots = align_up((uint32_t)(est_mean * 1.3 / 0.75) + 1, 32);
+  slots = std::min<uint32_t>(slots, ((budget - base) / 4) & ~31u);
+  if (const uint32_t hl = env_u32("DK_HASH_LOG2", 0)) slots = 1u << std::min<uint32_t>(hl, 16);
+  slots = std::max<uint32_t>(slots, 64);
+  P.hash_slots = slots;
+  P.hash_limit = slots * 3 / 4;
+  P.hash_log2 = log2_at_least(slots, 6, 16);  // only sizes the shared-memory carve-up below
+  P.warp_smem = base + align_up(slots * 4, 16);
+  plan_query_smem(P, pq, false);
+  P.off_hash = base;
+  if (P.warp_smem > (uint32_t)max_optin) return too_big();
+  P.gtable_log2 = log2_at_least(std::max(est, 2.0 * P.hash_limit) / 0.75, 10, 22);
+  P.gtable_log2 = std::min<uint32_t>(std::max<uint32_t>(env_u32("DK_GTABLE_LOG2", P.gtable_log2), 6), 24);
+  P.gtable_limit = (uint32_t)((1u << P.gtable_log2) * 0.75);
+  // Warps per CTA: the packing with the most resident warps per SM.
+  int best_warps = 0;
+  for (uint32_t wpc : {4u, 2u, 1u}) {
+    if (P.warp_smem * wpc > (uint32_t)max_optin) continue;
+    LaunchPlan Q{};
+    Q.kind = KernelKind::kWarp;
+    Q.p1 = P;
+    Q.score_u = L.score_u;
+    Q.warps_per_cta = wpc;
+    Q.query_only = true;
+    const cudaError_t e = dispatch(ix->metric, Q, mode, stream);
+    if (e != cudaSuccess) {
+      dk_set_error(DK_ERR_CUDA, std::string("occupancy query: ") + cudaGetErrorString(e));
+      return DK_ERR_CUDA;
+    }
+    if (Q.blocks_per_sm * (int)wpc > best_warps) {
+      best_warps = Q.blocks_per_sm * (int)wpc;
+      L.warps_per_cta = wpc;
+      L.blocks_per_sm = Q.blocks_per_sm;
+    }
+  }
+  if (best_warps == 0) return too_big();
+  const uint64_t want = (max_warps + L.warps_per_cta - 1) / L.warps_per_cta;
+  L.grid = (uint32_t)std::min<uint64_t>(want, (uint64_t)L.blocks_per_sm * (uint64_t)sms);
+  return DK_OK;
+}
+
+}  // namespace dk
+
+int32_t dk_launch_search(dk_index* ix, int32_t strategy, const float* queries,
+                         uint64_t qstride, uint32_t nq, uint32_t k, uint32_t l, uint32_t beam,
+                         uint32_t* ids, float* dists, dk_search_stats* stats,
+                         cudaStream_t stream) {
+  if (nq == 0) return DK_OK;
+  const int mode = mode_of_strategy(strategy);
+  const bool pq = mode == kModePQ;
+  SearchParams P{};
+  dk::base_params(ix, strategy, k, l, beam, P);
+  P.queries = queries;
+  P.qstride = qstride;
+  P.nq = nq;
+  P.out_ids = ids;
+  P.out_dists = dists;
+  P.stats = stats;
+  P.hint = ix->hint_dev;
+  double est = 0, est_mean = 0;
+  dk::visited_estimates(ix, P, est, est_mean);
 
   int dev = 0, max_optin = 0, sms = 0;
   cudaGetDevice(&dev);
@@ -144,50 +209,9 @@ int32_t dk_launch_search(dk_index* ix, int32_t strategy, const float* queries,
   uint64_t gtable_bytes = 0;
   cudaError_t e = cudaSuccess;
   if (warp) {
-    // Shared level: room for 1.3x the mean visited set at <= 3/4 load, within a per-warp
-    // shared-memory budget; the global level takes what a longer search adds.
     L.kind = dk::KernelKind::kWarp;
-    P.hash_log2 = 0;
-    const uint32_t base = plan_query_smem(P, pq, false);
-    const uint32_t budget = std::max<uint32_t>(env_u32("DK_WARP_SMEM", 24576), base + 1024);
-    uint32_t slots = align_up((uint32_t)(est_mean * 1.3 / 0.75) + 1, 32);
-    slots = std::min<uint32_t>(slots, ((budget - base) / 4) & ~31u);
-    if (const uint32_t hl = env_u32("DK_HASH_LOG2", 0)) slots = 1u << std::min<uint32_t>(hl, 16);
-    slots = std::max<uint32_t>(slots, 64);
-    P.hash_slots = slots;
-    P.hash_limit = slots * 3 / 4;
-    P.hash_log2 = log2_at_least(slots, 6, 16);  // only sizes the shared-memory carve-up below
-    P.warp_smem = base + align_up(slots * 4, 16);
-    plan_query_smem(P, pq, false);
-    P.off_hash = base;
-    if (P.warp_smem > (uint32_t)max_optin) return too_big();
-    P.gtable_log2 = log2_at_least(std::max(est, 2.0 * P.hash_limit) / 0.75, 10, 22);
-    P.gtable_log2 = std::min<uint32_t>(std::max<uint32_t>(env_u32("DK_GTABLE_LOG2", P.gtable_log2), 6), 24);
-    P.gtable_limit = (uint32_t)((1u << P.gtable_log2) * 0.75);
-    // Warps per CTA: the packing with the most resident warps per SM.
-    int best_warps = 0;
-    for (uint32_t wpc : {4u, 2u, 1u}) {
-      if (P.warp_smem * wpc > (uint32_t)max_optin) continue;
-      dk::LaunchPlan Q{};
-      Q.kind = dk::KernelKind::kWarp;
-      Q.p1 = P;
-      Q.score_u = L.score_u;
-      Q.warps_per_cta = wpc;
-      Q.query_only = true;
-      e = dispatch(ix->metric, Q, mode, stream);
-      if (e != cudaSuccess) {
-        dk_set_error(DK_ERR_CUDA, std::string("occupancy query: ") + cudaGetErrorString(e));
-        return DK_ERR_CUDA;
-      }
-      if (Q.blocks_per_sm * (int)wpc > best_warps) {
-        best_warps = Q.blocks_per_sm * (int)wpc;
-        L.warps_per_cta = wpc;
-        L.blocks_per_sm = Q.blocks_per_sm;
-      }
-    }
-    if (best_warps == 0) return too_big();
-    const uint32_t want = (nq + L.warps_per_cta - 1) / L.warps_per_cta;
-    L.grid = std::min<uint32_t>(want, (uint32_t)L.blocks_per_sm * (uint32_t)sms);
+    const int32_t rc = dk::plan_warp(ix, P, L, mode, est, est_mean, nq, stream);
+    if (rc != DK_OK) return rc;
     gtable_bytes = (uint64_t)L.grid * L.warps_per_cta * (4ull << P.gtable_log2);
   } else {
     L.kind = dk::KernelKind::kCta;
@@ -196,7 +220,7 @@ int32_t dk_launch_search(dk_index* ix, int32_t strategy, const float* queries,
     P.hash_log2 = std::min<uint32_t>(std::max<uint32_t>(log2h, 6), 20);
     while (true) {
       P.hash_limit = (uint32_t)((1u << P.hash_log2) * 0.75);
-      P.smem_bytes = plan_query_smem(P, pq, true);
+      P.smem_bytes = dk::plan_query_smem(P, pq, true);
       if (P.smem_bytes <= (uint32_t)max_optin) break;
       if (P.hash_log2 <= 6) return too_big();
       --P.hash_log2;
@@ -205,7 +229,7 @@ int32_t dk_launch_search(dk_index* ix, int32_t strategy, const float* queries,
 
   SearchParams P2 = P;
   P2.hash_limit = 0xFFFFFFFFu;  // the bitmap never fills
-  P2.smem_bytes = plan_query_smem(P2, pq, false);
+  P2.smem_bytes = dk::plan_query_smem(P2, pq, false);
   if (P2.smem_bytes > (uint32_t)max_optin) return too_big();
 
   // Scratch, one stream-ordered allocation: work counter | global tables | spill bitmaps.
@@ -218,9 +242,9 @@ int32_t dk_launch_search(dk_index* ix, int32_t strategy, const float* queries,
   const uint64_t off_bitmap = align_up64(off_gtable + gtable_bytes, 256);
   const uint64_t total = off_bitmap + per * spill_ctas;
   unsigned char* scratch = nullptr;
-  e = cudaMallocAsync(reinterpret_cast<void**>(&scratch), total, stream);
+  e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&scratch), total, ix->pool, stream);
   if (e != cudaSuccess) {
-    dk_set_error(DK_ERR_OUT_OF_MEMORY, std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
+    dk_set_error(DK_ERR_OUT_OF_MEMORY, std::string("scratch allocation: ") + cudaGetErrorString(e));
     return DK_ERR_OUT_OF_MEMORY;
   }
   e = cudaMemsetAsync(scratch, 0, 256, stream);
@@ -231,7 +255,7 @@ int32_t dk_launch_search(dk_index* ix, int32_t strategy, const float* queries,
   L.p1 = P;
   L.p2 = P2;
   L.spill_ctas = spill_ctas;
-  if (e == cudaSuccess) e = dispatch(ix->metric, L, mode, stream);
+  if (e == cudaSuccess) e = dk::dispatch(ix->metric, L, mode, stream);
   cudaFreeAsync(scratch, stream);
   // Stage this launch's visited-size statistics for the next launch's planning, then reset.
   if (e == cudaSuccess)

@@ -55,6 +55,7 @@ class Status(enum.IntEnum):
     CANCELLED = 14
     NOT_FOUND = 15
     NO_LOW_PRECISION = 16
+    NOT_READY = 17
 
 
 class ANNError(RuntimeError):
@@ -265,3 +266,81 @@ class DiskANNIndex:
             params.k_value, params.l_value, params.beam_width, ids.data_ptr(), dists.data_ptr(),
             stats.data_ptr(), ctypes.c_void_p(handle),
         ))
+
+
+class SearchServer:
+    """Continuous-admission serving over a :class:`GpuProvider` (``dk_server_*``).
+
+    ``submit`` queues one request with its own ``k`` and ``L`` (up to ``max_k`` / ``max_l``)
+    and returns a ticket; queued requests are launched as soon as one of ``streams`` launch
+    contexts is free, overlapping on the device with requests already running.  ``poll``
+    returns ``(ids, dists, stats)`` once the request is done, else ``None``.  A submit while
+    ``queue_depth`` requests are outstanding raises ``ANNError`` with status ``ADMISSION``.
+    """
+
+    def __init__(self, provider: GpuProvider, strategy: _Strategy, max_k: int, max_l: int,
+                 beam_width: int = 1, queue_depth: int = 1024, max_slots: int = 0,
+                 streams: int = 0):
+        L = _native.load()
+        cfg = _native.ServerConfig(strategy.code, max_k, max_l, beam_width, queue_depth,
+                                   max_slots, streams)
+        handle = ctypes.c_void_p()
+        _check(L.dk_server_create(provider.handle, ctypes.byref(cfg), ctypes.byref(handle)))
+        self._handle = handle
+        self.provider = provider
+        self.max_k = int(max_k)
+
+    @property
+    def handle(self):
+        if self._handle is None:
+            raise ANNError(Status.INVALID_ARGUMENT, "server is closed")
+        return self._handle
+
+    def submit(self, query, k: int, l_value: int) -> int:
+        q = np.ascontiguousarray(np.ravel(query), dtype=np.float32)
+        if q.shape[0] != self.provider.dim:
+            raise ANNError(Status.DIMENSION_MISMATCH, f"query dim {q.shape[0]} != {self.provider.dim}")
+        ticket = ctypes.c_uint64()
+        _check(_native.load().dk_server_submit(self.handle, q.ctypes.data, k, l_value,
+                                               ctypes.byref(ticket)))
+        return int(ticket.value)
+
+    def poll(self, ticket: int, k: int):
+        ids = np.empty(k, dtype=np.uint32)
+        dists = np.empty(k, dtype=np.float32)
+        stats = np.zeros(1, dtype=STATS_DTYPE)
+        rc = _native.load().dk_server_poll(self.handle, ticket, ids.ctypes.data,
+                                           dists.ctypes.data, stats.ctypes.data)
+        if rc == Status.NOT_READY:
+            return None
+        _check(rc)
+        return ids, dists, stats[0]
+
+    def wait(self, ticket: int, k: int, timeout_s: float = 30.0):
+        """Poll until the request completes (``TimeoutError`` after ``timeout_s``)."""
+        import time
+
+        deadline = time.monotonic() + timeout_s
+        while True:
+            r = self.poll(ticket, k)
+            if r is not None:
+                return r
+            if time.monotonic() > deadline:
+                raise TimeoutError(f"request {ticket} not done after {timeout_s} s")
+            time.sleep(0)
+
+    def info(self) -> dict:
+        inf = _native.ServerInfo()
+        _check(_native.load().dk_server_get_info(self.handle, ctypes.byref(inf)))
+        return {f: getattr(inf, f) for f, _ in inf._fields_ if f != "pad"}
+
+    def close(self) -> None:
+        if getattr(self, "_handle", None) is not None:
+            _native.load().dk_server_destroy(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -161,35 +161,41 @@ int32_t dk_search_device(dk_index* index, int32_t strategy, const float* queries
                          dk_search_stats* stats, void* stream);
 
 
-/* ---- Serving: a persistent device loop with continuous admission (no counterpart in the
- * reference, whose searches are one call per query on host tasks) ----
+/* ---- Serving: continuous admission of single requests (no counterpart in the reference,
+ * whose searches are one async call per query scheduled by the caller's runtime) ----
  *
- * dk_server_create starts a device loop whose warps each own one search slot (shared-memory
- * beam state and a visited set sized for max_l).  dk_server_submit copies one request into a
- * ring in pinned host memory and publishes it; a free slot on the device claims it while
- * other requests are in flight, so requests of different k and L overlap on the GPU.
- * dk_server_poll returns DK_OK once the request's results are in the caller's buffers, or
- * DK_ERR_NOT_READY.  Admission: a submit is rejected with DK_ERR_ADMISSION when
- * queue_depth requests are outstanding; slots are sized from shared memory and device
- * memory at creation.  Every device-side wait is bounded: the loop exits after idle_ms
- * without work (the next submit or poll restarts it) and when the server is destroyed. */
+ * dk_server_submit queues one request (its own k and L, up to max_k / max_l) and returns a
+ * ticket.  Queued requests are launched as soon as one of the server's `streams` launch
+ * contexts is free: a request that arrives while others are on the GPU goes out in the next
+ * launch on another stream, and the launches overlap on the device (each a warp-per-request
+ * search whose beam state and visited set stay in shared memory and HBM for the whole
+ * search).  Requests that arrive while every context is busy are launched together when the
+ * first one frees up.  dk_server_poll returns DK_OK once the request's results are in the
+ * caller's buffers, else DK_ERR_NOT_READY; polling also reaps finished launches and starts
+ * queued ones.  Admission: a submit is rejected with DK_ERR_ADMISSION while queue_depth
+ * requests are outstanding (submitted, not yet collected).  All device memory (per-context
+ * query, result and visited-table buffers) is taken at creation, sized from max_l, the
+ * contexts' slots and the free device memory; no device code waits on the host.
+ * A server's calls are serialised by an internal lock. */
 typedef struct dk_server dk_server;
 
 typedef struct dk_server_config {
   int32_t strategy;      /* enum dk_strategy, for every request */
   uint32_t max_k;        /* per-request k <= max_k */
   uint32_t max_l;        /* per-request L <= max_l */
-  uint32_t beam_width;   /* for every request */
-  uint32_t queue_depth;  /* outstanding requests accepted (ring size) */
-  uint32_t max_slots;    /* device slots (0 = as many as fit) */
-  uint32_t idle_ms;      /* device loop exits after this long without work (0 = 200) */
+  uint32_t beam_width;   /* for every request (<= 4) */
+  uint32_t queue_depth;  /* outstanding requests accepted */
+  uint32_t max_slots;    /* concurrent searches per launch (0 = all resident warps) */
+  uint32_t streams;      /* launch contexts that overlap on the device (0 = 4) */
 } dk_server_config;
 
 typedef struct dk_server_info {
-  uint32_t slots;            /* concurrent searches on the device */
+  uint32_t slots;            /* concurrent searches per launch */
   uint32_t queue_depth;
-  uint64_t device_bytes;     /* HBM held by the server (visited-set tables, ring state) */
-  uint64_t launches;         /* device-loop launches so far */
+  uint32_t streams;
+  uint32_t pad;
+  uint64_t device_bytes;     /* HBM held by the server */
+  uint64_t launches;         /* kernel launches so far */
 } dk_server_info;
 
 int32_t dk_server_create(dk_index* index, const dk_server_config* config, dk_server** out);
