@@ -24,6 +24,7 @@ EXPORTED_SYMBOLS = (
     "dk_index_get_info",
     "dk_search",
     "dk_search_device",
+    "dk_search_device_noalloc",
     "dk_server_create",
     "dk_server_submit",
     "dk_server_poll",
@@ -131,6 +132,8 @@ def load():
         L.dk_search.argtypes = [vp, i32, vp, u64, u32, u32, u32, u32, vp, vp, vp]
         L.dk_search_device.restype = i32
         L.dk_search_device.argtypes = [vp, i32, vp, u64, u32, u32, u32, u32, vp, vp, vp, vp]
+        L.dk_search_device_noalloc.restype = i32
+        L.dk_search_device_noalloc.argtypes = [vp, i32, vp, u64, u32, u32, u32, u32, vp, vp, vp, vp]
         L.dk_server_create.restype = i32
         L.dk_server_create.argtypes = [vp, ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]
         L.dk_server_submit.restype = i32

@@ -160,6 +160,29 @@ int32_t dk_search_device(dk_index* index, int32_t strategy, const float* queries
                          uint32_t beam_width, uint32_t* ids, float* dists,
                          dk_search_stats* stats, void* stream);
 
+/* Same search, arguments and results as dk_search_device, for callers that cannot allocate
+ * device memory while they search: for example a process whose own caching allocator took the
+ * GPU's free memory at start-up (so the allocation inside dk_search_device would fail), or a
+ * latency-critical path that must not enter the CUDA allocator.  This entry point allocates
+ * nothing: its scratch (work counter, per-warp visited tables, spill bitmaps) comes from one
+ * fixed device array of DK_NOALLOC_SCRATCH_BYTES that the library declares statically, which
+ * every GPU that loads the library holds until the process exits.  No counterpart in the
+ * reference.
+ *  - Set-up: the first call on a device, made with that device current, looks up the array's
+ *    device address; make that first call (nq = 0 is enough) before any stream capture.
+ *  - Limit: a search whose scratch would not fit the array (one spill bitmap of (N+F)/8
+ *    bytes plus one CTA's visited tables at least) is refused with DK_ERR_UNSUPPORTED and a
+ *    message giving the bytes it needs; large batches run with fewer warps when not all of
+ *    their tables fit.
+ *  - Every call on a device shares the array and it keeps the last call's contents; each call
+ *    clears what must start at zero.  Calls whose work overlaps on the GPU race on the array:
+ *    issue them on one stream, or let one finish before the next starts. */
+#define DK_NOALLOC_SCRATCH_BYTES (32u << 20)
+int32_t dk_search_device_noalloc(dk_index* index, int32_t strategy, const float* queries,
+                                 uint64_t query_stride, uint32_t nq, uint32_t k, uint32_t l,
+                                 uint32_t beam_width, uint32_t* ids, float* dists,
+                                 dk_search_stats* stats, void* stream);
+
 
 /* ---- Serving: continuous admission of single requests (no counterpart in the reference,
  * whose searches are one async call per query scheduled by the caller's runtime) ----
