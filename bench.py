@@ -24,7 +24,6 @@ import argparse
 import hashlib
 import json
 import os
-import subprocess
 import sys
 import time
 
@@ -114,56 +113,77 @@ def prepare(name: str, rank: int, cache_root: str):
 
 
 class ClockSampler:
-    """nvidia-smi clocks sampled every 200 ms while the timed region runs."""
+    """SM clock and clock-event reasons sampled through NVML every 5 ms while the timed region
+    runs (the fields of nvidia-smi's clocks line); read-only queries, no settings touched."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"),
+               ("hw_power_brake_slowdown", "nvmlClocksEventReasonHwPowerBrakeSlowdown"))
 
-    def __init__(self, device_index: int):
+    def __init__(self, device_index: int, period_s: float = 0.005):
         self.dev = device_index
-        self.proc = None
-        self.path = f"/tmp/dk_clocks_{os.getpid()}.csv"
+        self.period = period_s
+        self.samples = []
+        self.max_mhz = None
+        self.error = None
+        self._stop = None
+        self._thread = None
+
+    def _handle(self, nv):
+        import torch
+
+        try:
+            p = torch.cuda.get_device_properties(self.dev)
+            bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+            return nv.nvmlDeviceGetHandleByPciBusId(bus.encode())
+        except Exception:
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+            ids = [x for x in vis.split(",") if x.strip().isdigit()]
+            return nv.nvmlDeviceGetHandleByIndex(int(ids[self.dev]) if self.dev < len(ids) else self.dev)
 
     def __enter__(self):
+        import threading
+
         try:
-            self.f = open(self.path, "w")
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
-                stdout=self.f, stderr=subprocess.DEVNULL)
-        except Exception:
-            self.proc = None
+            import pynvml as nv
+
+            nv.nvmlInit()
+            h = self._handle(nv)
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            masks = [(name, getattr(nv, attr)) for name, attr in self.REASONS]
+            self._stop = threading.Event()
+
+            def run():
+                while not self._stop.is_set():
+                    try:
+                        mhz = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                        r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                        self.samples.append((float(mhz), [n for n, m in masks if r & m]))
+                    except Exception as e:  # keep the timed region going
+                        self.error = str(e)
+                    self._stop.wait(self.period)
+
+            self._thread = threading.Thread(target=run, daemon=True)
+            self._thread.start()
+        except Exception as e:
+            self.error = str(e)
         return self
 
     def __exit__(self, *exc):
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except Exception:
-                self.proc.kill()
-            self.f.close()
+        if self._thread is not None:
+            self._stop.set()
+            self._thread.join(timeout=5)
 
     def summary(self):
-        rows = []
-        try:
-            with open(self.path) as f:
-                for line in f:
-                    p = [x.strip() for x in line.split(",")]
-                    if len(p) >= 9:
-                        rows.append(p)
-            os.remove(self.path)
-        except Exception:
-            pass
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
-        return {"sm_mhz": float(np.median(sm)) if sm else None,
-                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"],
+                    "samples": 0, "error": self.error}
+        sm = [m for m, _ in self.samples]
+        reasons = sorted({n for _, rs in self.samples for n in rs})
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                "samples": len(self.samples), "source": "NVML, 5 ms period"}
 
 
 STRATEGY_CODES = ("fp32", "bf16", "fp8", "hybrid")
@@ -477,6 +497,31 @@ def config_of(w, name, l, strategy):
     }
 
 
+def profile_case(args):
+    """Two searches of the workload's query batch with one strategy and L (for ncu -s 1 -c 1)."""
+    import torch
+
+    from diskann_b200 import DiskANNIndex, GpuProvider, Knn, Metric
+
+    name, l = args.profile.split(":")
+    data = prepare(args.workload, 0, args.cache)
+    w = data["w"]
+    torch.cuda.set_device(0)
+    prov = GpuProvider(data["vectors"], data["adj"], data["deg"], data["n"], Metric.L2,
+                       pq=data["pq"], low_precision=("bf16", "fp8"))
+    idx = DiskANNIndex(prov)
+    q = torch.from_numpy(data["queries"]).cuda()
+    nq, k = q.shape[0], w["k"]
+    ids = torch.empty((nq, k), dtype=torch.int32, device="cuda")
+    dists = torch.empty((nq, k), dtype=torch.float32, device="cuda")
+    stats = torch.empty((nq, 4), dtype=torch.int32, device="cuda")
+    for _ in range(2):
+        idx.search_device(Knn(k, int(l)), strategy_objects()[name], q, ids, dists, stats)
+    torch.cuda.synchronize()
+    log(f"[profile] {name} L={l}: mean cmps {float(stats[:, 0].float().mean()):.1f}")
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -488,12 +533,18 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--serve-seconds", type=float, default=2.0)
+    ap.add_argument("--profile", default=None, metavar="STRATEGY:L",
+                    help="profiling case for ncu: upload the workload's index and run two "
+                         "batched searches (warm-up, profiled), no timing, no JSON line")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     threads = os.cpu_count() or 1
+
+    if args.profile:
+        return profile_case(args)
 
     if args.impl == "reference":
         # The reference's search on the host cores: the oracle port (the reference is Rust and

@@ -44,7 +44,8 @@ void free_index(dk_index* ix) {
   cudaFree(ix->offsets);
   cudaFree(ix->vec_bf16);
   cudaFree(ix->vec_fp8);
-  cudaFree(ix->fp8_scale);
+  cudaFree(ix->bf16_meta);
+  cudaFree(ix->fp8_meta);
   cudaFree(ix->hint_dev);
   if (ix->hint_stage) cudaFreeHost(ix->hint_stage);
   if (ix->pool) cudaMemPoolDestroy(ix->pool);

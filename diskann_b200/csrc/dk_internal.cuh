@@ -26,10 +26,12 @@ struct dk_index {
   float* pivots = nullptr;
   float* pivots_cm = nullptr;  // chunk-major copy: chunk m, centre c -> len_m floats
   uint32_t* offsets = nullptr;
-  // Low-precision copies: rows of lp_stride elements (a multiple of 16, zero padded).
-  uint16_t* vec_bf16 = nullptr;   // BF16 bit patterns
-  uint8_t* vec_fp8 = nullptr;     // FP8-E4M3, value = fp8 * fp8_scale[row]
-  float* fp8_scale = nullptr;
+  // Low-precision copies: rows of lp_stride elements (a multiple of 16, zero padded), each
+  // with (scale, squared norm of the de-quantised row) in the matching *_meta array.
+  uint16_t* vec_bf16 = nullptr;   // BF16 bit patterns (scale 1)
+  uint8_t* vec_fp8 = nullptr;     // FP8-E4M3, value = fp8 * scale
+  float2* bf16_meta = nullptr;
+  float2* fp8_meta = nullptr;
   uint32_t lp_stride = 0;
   uint64_t bytes = 0;
   // Visited-set sizing hint, in units of cmps * 256 / (L + F).  Kernels update three device
@@ -57,7 +59,8 @@ struct SearchParams {
   const uint32_t* offsets;
   const uint16_t* vec_bf16;
   const uint8_t* vec_fp8;
-  const float* fp8_scale;
+  const float2* bf16_meta;
+  const float2* fp8_meta;
   uint32_t lp_stride;
   uint32_t n, f, dim, vstride, astride, max_degree, cstride, pq_chunks;
   const float* queries;

@@ -119,23 +119,36 @@ struct WarpVisited {
   uint32_t scount = 0;  // ids in the shared level
   uint32_t gcount = 0;  // ids in the global level
 
-  __device__ void reset(uint32_t lane) {
+  __device__ __forceinline__ void reset(uint32_t lane) {
     for (uint32_t i = lane; i < ssize; i += 32u) s[i] = kEmpty;
     scount = 0u;
     gcount = 0u;
   }
   __device__ __forceinline__ uint32_t next(uint32_t h) const { return h + 1 == ssize ? 0u : h + 1; }
-  // Every lane calls; lanes with `want` test-and-insert their `id`.  True if it was new.
-  __device__ bool insert(bool want, uint32_t id) {
+  // Shared-level half of an insert.  Every lane calls; lanes with `want` test `id`.  Returns
+  // true if the id was new and went into the shared level; `global` is set when the id is not
+  // in the frozen shared level and must be tested against the global level.
+  // The shared level probes linearly, four slots (one 16-byte bucket) per read: slots fill in
+  // probe order and nothing is ever removed, so the first empty slot ends a lookup.
+  __device__ __forceinline__ bool shared_step(bool want, uint32_t id, bool& global) {
     volatile uint32_t* vs = s;
     bool present = false;
-    uint32_t h = __umulhi(id * 2654435761u, ssize);
+    const uint32_t nbk = ssize >> 2;
+    uint32_t b = __umulhi(id * 2654435761u, nbk);
+    uint32_t h = 0;
     if (want) {
+      const uint32_t base = (uint32_t)__cvta_generic_to_shared(s);
       while (true) {
-        const uint32_t cur = vs[h];
-        if (cur == id) { present = true; break; }
-        if (cur == kEmpty) break;
-        h = next(h);
+        uint32_t v0, v1, v2, v3;
+        asm volatile("ld.volatile.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
+                     : "=r"(v0), "=r"(v1), "=r"(v2), "=r"(v3)
+                     : "r"(base + 16u * b));
+        if (v0 == id || v1 == id || v2 == id || v3 == id) { present = true; break; }
+        if (v0 == kEmpty) { h = 4u * b; break; }
+        if (v1 == kEmpty) { h = 4u * b + 1u; break; }
+        if (v2 == kEmpty) { h = 4u * b + 2u; break; }
+        if (v3 == kEmpty) { h = 4u * b + 3u; break; }
+        b = b + 1u == nbk ? 0u : b + 1u;
       }
     }
     const bool absent = want && !present;
@@ -151,20 +164,62 @@ struct WarpVisited {
       fresh = true;
     }
     scount += min((uint32_t)__popc(m), room);
-    const bool global = absent && rank >= room;
+    global = absent && rank >= room;
+    return fresh;
+  }
+
+  __device__ __forceinline__ uint32_t ghash(uint32_t id) const {
+    return ((id ^ 0x5bd1e995u) * 0x9E3779B1u) >> gshift;
+  }
+
+  // Global-level probe continued from the id's home slot, whose CAS returned `old`: true if
+  // `id` was new.
+  __device__ __forceinline__ bool global_finish(uint32_t id, uint32_t old) {
+    uint32_t hg = ghash(id);
+    while (true) {
+      if (old == kEmpty) return true;
+      if (old == id) return false;
+      hg = (hg + 1) & gmask;
+      old = atomicCAS(&g[hg], kEmpty, id);  // one round trip per step
+    }
+  }
+
+  // Every lane calls; lanes with `want` test-and-insert their `id`.  True if it was new.
+  __device__ __forceinline__ bool insert(bool want, uint32_t id) {
+    bool global;
+    bool fresh = shared_step(want, id, global);
     if (__any_sync(kFull, global)) {
       if (global) {
-        uint32_t hg = ((id ^ 0x5bd1e995u) * 0x9E3779B1u) >> gshift;
-        while (true) {
-          const uint32_t old = atomicCAS(&g[hg], kEmpty, id);  // one round trip per step
-          if (old == kEmpty) { fresh = true; break; }
-          if (old == id) break;
-          hg = (hg + 1) & gmask;
-        }
+        fresh = global_finish(id, atomicCAS(&g[ghash(id)], kEmpty, id));
       }
       gcount += __popc(__ballot_sync(kFull, global && fresh));
     }
     return fresh;
+  }
+
+  // The ids of one adjacency row, up to 128, lane `l` holding entries l, l+32, l+64, l+96:
+  // the shared level is updated round by round (in row order), then the first global-level
+  // probes of all rounds are issued together, so a row costs one global round trip, not one
+  // per round.  Ids of one row are distinct.
+  __device__ __forceinline__ void insert_row(const uint32_t (&id)[4], uint32_t deg, uint32_t lane,
+                                             bool (&fresh)[4]) {
+    bool glob[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      glob[r] = false;
+      fresh[r] = false;
+      if (32u * r < deg) fresh[r] = shared_step(32u * r + lane < deg, id[r], glob[r]);
+    }
+    if (__any_sync(kFull, glob[0] || glob[1] || glob[2] || glob[3])) {
+      uint32_t old[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) old[r] = glob[r] ? atomicCAS(&g[ghash(id[r])], kEmpty, id[r]) : kEmpty;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        if (glob[r]) fresh[r] = global_finish(id[r], old[r]);
+        gcount += __popc(__ballot_sync(kFull, glob[r] && fresh[r]));
+      }
+    }
   }
 };
 
@@ -443,6 +498,70 @@ __device__ __forceinline__ void fp8x16(const uint4 w, float (&x)[16]) {
   }
 }
 
+// Low-precision distance from the row's dot product with the query and its (scale, norm):
+// L2 |q|^2 + norm - 2 s (q.x); inner product -s (q.x); normalised cosine 1 - s (q.x); cosine
+// 1 - clamp(s (q.x) / (|q| sqrt(norm))), similarity 0 if a norm is below f32::MIN_POSITIVE.
+template <int METRIC>
+__device__ __forceinline__ float lp_distance(float dot, float2 meta, float qq) {
+  const float sd = meta.x * dot;
+  if (METRIC == DK_METRIC_L2) return __fmaf_rn(-2.0f, sd, qq + meta.y);
+  if (METRIC == DK_METRIC_INNER_PRODUCT) return -sd;
+  if (METRIC == DK_METRIC_COSINE_NORMALIZED) return 1.0f - sd;
+  if (qq < 1.17549435e-38f || meta.y < 1.17549435e-38f) return 1.0f;
+  return 1.0f - fmaxf(-1.0f, fminf(1.0f, sd / (sqrtf(qq) * sqrtf(meta.y))));
+}
+
+// |q|^2 over the pieces lane s of a subgroup owns (pieces s, s+8, ...), summed over the 8 lanes.
+template <uint32_t kPer>
+__device__ __forceinline__ float subgroup_qq(const float* q, uint32_t pieces, uint32_t s,
+                                            unsigned gmask) {
+  float qq = 0.0f;
+  for (uint32_t p = s; p < pieces; p += 8u) {
+    const float4* q4 = reinterpret_cast<const float4*>(q + p * kPer);
+#pragma unroll
+    for (uint32_t i = 0; i < kPer / 4; ++i) {
+      const float4 t = q4[i];
+      qq = __fmaf_rn(t.x, t.x, qq);
+      qq = __fmaf_rn(t.y, t.y, qq);
+      qq = __fmaf_rn(t.z, t.z, qq);
+      qq = __fmaf_rn(t.w, t.w, qq);
+    }
+  }
+#pragma unroll
+  for (int o = 1; o < 8; o <<= 1) qq += __shfl_xor_sync(gmask, qq, o, 8);
+  return qq;
+}
+
+// Dot product of one 16-byte piece of a low-precision row with the matching query floats.
+template <int MODE>
+__device__ __forceinline__ float piece_dot(uint4 w, const float* qp, float acc) {
+  constexpr uint32_t kPer = MODE == kModeBF16 ? 8u : 16u;
+  float x[kPer];
+  if (MODE == kModeBF16) bf16x8(w, *reinterpret_cast<float(*)[8]>(x));
+  else fp8x16(w, *reinterpret_cast<float(*)[16]>(x));
+  const float4* q4 = reinterpret_cast<const float4*>(qp);
+#pragma unroll
+  for (uint32_t i = 0; i < kPer / 4; ++i) {
+    const float4 t = q4[i];
+    acc = __fmaf_rn(t.x, x[4 * i], acc);
+    acc = __fmaf_rn(t.y, x[4 * i + 1], acc);
+    acc = __fmaf_rn(t.z, x[4 * i + 2], acc);
+    acc = __fmaf_rn(t.w, x[4 * i + 3], acc);
+  }
+  return acc;
+}
+
+template <int MODE>
+__device__ __forceinline__ const unsigned char* lp_rows(const SearchParams& P) {
+  return MODE == kModeBF16 ? reinterpret_cast<const unsigned char*>(P.vec_bf16)
+                           : reinterpret_cast<const unsigned char*>(P.vec_fp8);
+}
+
+template <int MODE>
+__device__ __forceinline__ const float2* lp_meta(const SearchParams& P) {
+  return MODE == kModeBF16 ? P.bf16_meta : P.fp8_meta;
+}
+
 template <int METRIC, int MODE, int U>
 __device__ __forceinline__ void score_lp(const SearchParams& P, const float* q, const uint32_t* ids,
                                          float* d, uint32_t count, uint32_t sg, uint32_t nsub,
@@ -450,81 +569,113 @@ __device__ __forceinline__ void score_lp(const SearchParams& P, const float* q, 
   constexpr uint32_t kPer = MODE == kModeBF16 ? 8u : 16u;  // elements per 16-byte piece
   const uint32_t pieces = P.lp_stride / kPer;
   const uint32_t row_bytes = P.lp_stride * (MODE == kModeBF16 ? 2u : 1u);
-  const unsigned char* base = MODE == kModeBF16
-                                  ? reinterpret_cast<const unsigned char*>(P.vec_bf16)
-                                  : reinterpret_cast<const unsigned char*>(P.vec_fp8);
+  const unsigned char* base = lp_rows<MODE>(P);
+  const float2* meta = lp_meta<MODE>(P);
+  const float qq = (METRIC == DK_METRIC_L2 || METRIC == DK_METRIC_COSINE)
+                       ? subgroup_qq<kPer>(q, pieces, s, gmask) : 0.0f;
   const uint32_t step = nsub * U;
   for (uint32_t b0 = 0; b0 < count; b0 += step) {
     const uint4* rows[U];
     uint32_t idx[U], rid[U];
-    float acc[U], yy[U], qq = 0.0f;
+    float acc[U];
+    float2 mt[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       idx[u] = b0 + sg + u * nsub;
       rid[u] = ids[idx[u] < count ? idx[u] : count - 1];
       rows[u] = reinterpret_cast<const uint4*>(base + (size_t)rid[u] * row_bytes);
+      mt[u] = __ldg(meta + rid[u]);
       acc[u] = 0.0f;
-      yy[u] = 0.0f;
     }
-    float scale[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) scale[u] = MODE == kModeFP8 ? __ldg(P.fp8_scale + rid[u]) : 1.0f;
     for (uint32_t p = s; p < pieces; p += 8u) {
       uint4 w[U];
 #pragma unroll
       for (int u = 0; u < U; ++u) w[u] = __ldg(rows[u] + p);
-      float qv[kPer];
-      const float4* q4 = reinterpret_cast<const float4*>(q + p * kPer);
 #pragma unroll
-      for (uint32_t i = 0; i < kPer / 4; ++i) {
-        const float4 t = q4[i];
-        qv[4 * i] = t.x; qv[4 * i + 1] = t.y; qv[4 * i + 2] = t.z; qv[4 * i + 3] = t.w;
-      }
-      if (METRIC == DK_METRIC_COSINE) {
-#pragma unroll
-        for (uint32_t i = 0; i < kPer; ++i) qq = __fmaf_rn(qv[i], qv[i], qq);
-      }
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        float x[kPer];
-        if (MODE == kModeBF16) bf16x8(w[u], *reinterpret_cast<float(*)[8]>(x));
-        else fp8x16(w[u], *reinterpret_cast<float(*)[16]>(x));
-#pragma unroll
-        for (uint32_t i = 0; i < kPer; ++i) {
-          if (METRIC == DK_METRIC_L2) {
-            const float c = qv[i] - scale[u] * x[i];
-            acc[u] = __fmaf_rn(c, c, acc[u]);
-          } else {
-            acc[u] = __fmaf_rn(qv[i], x[i], acc[u]);
-            if (METRIC == DK_METRIC_COSINE) yy[u] = __fmaf_rn(x[i], x[i], yy[u]);
-          }
-        }
-      }
+      for (int u = 0; u < U; ++u) acc[u] = piece_dot<MODE>(w[u], q + p * kPer, acc[u]);
     }
 #pragma unroll
     for (int o = 1; o < 8; o <<= 1) {
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        acc[u] += __shfl_xor_sync(gmask, acc[u], o, 8);
-        if (METRIC == DK_METRIC_COSINE) yy[u] += __shfl_xor_sync(gmask, yy[u], o, 8);
-      }
-      if (METRIC == DK_METRIC_COSINE) qq += __shfl_xor_sync(gmask, qq, o, 8);
+      for (int u = 0; u < U; ++u) acc[u] += __shfl_xor_sync(gmask, acc[u], o, 8);
     }
     if (s == 0) {
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        if (idx[u] >= count) continue;
-        float r;
-        if (METRIC == DK_METRIC_L2) r = acc[u];
-        else if (METRIC == DK_METRIC_INNER_PRODUCT) r = -scale[u] * acc[u];
-        else if (METRIC == DK_METRIC_COSINE_NORMALIZED) r = 1.0f - scale[u] * acc[u];
-        else {
-          const float den = sqrtf(qq) * sqrtf(yy[u]);
-          r = (qq < 1.17549435e-38f || yy[u] < 1.17549435e-38f) ? 1.0f
-              : 1.0f - fmaxf(-1.0f, fminf(1.0f, acc[u] / den));
-        }
-        d[idx[u]] = r;
+      for (int u = 0; u < U; ++u)
+        if (idx[u] < count) d[idx[u]] = lp_distance<METRIC>(acc[u], mt[u], qq);
+    }
+  }
+}
+
+// Row geometry of the low-precision copies for a compile-time dimension: 16-byte pieces per
+// row, pieces each lane of an 8-lane subgroup loads per row (kNP), and rows per subgroup per
+// round (kU) chosen so a lane has about eight 16-byte loads in flight.
+template <int MODE, int DIM>
+struct LpShape {
+  static constexpr uint32_t kPer = MODE == kModeBF16 ? 8u : 16u;
+  static constexpr uint32_t kStride = (uint32_t)(DIM + 15) / 16u * 16u;
+  static constexpr uint32_t kPieces = kStride / kPer;
+  static constexpr uint32_t kNP = (kPieces + 7u) / 8u;
+  static constexpr int kU = kNP >= 8u ? 1 : (int)(8u / kNP);
+};
+
+// score_lp for a compile-time dimension, in wide rounds: every 16-byte piece of a round's rows
+// (kU rows per subgroup) and their (scale, norm) are requested before the first conversion, so
+// a hop's ~40 FP8 rows cost two memory latencies instead of five.  Per-lane sums and the
+// butterfly run in the same order as score_lp, so both give identical distances.
+template <int METRIC, int MODE, int DIM>
+__device__ __forceinline__ void score_lp_wide(const SearchParams& P, const float* q,
+                                              const uint32_t* ids, float* d, uint32_t count,
+                                              uint32_t sg, uint32_t nsub, uint32_t s,
+                                              unsigned gmask) {
+  using Sh = LpShape<MODE, DIM>;
+  constexpr uint32_t kPer = Sh::kPer;
+  constexpr int U = Sh::kU;
+  constexpr int NP = (int)Sh::kNP;
+  constexpr uint32_t row_bytes = Sh::kStride * (MODE == kModeBF16 ? 2u : 1u);
+  const unsigned char* base = lp_rows<MODE>(P);
+  const float2* meta = lp_meta<MODE>(P);
+  const float qq = (METRIC == DK_METRIC_L2 || METRIC == DK_METRIC_COSINE)
+                       ? subgroup_qq<kPer>(q, Sh::kPieces, s, gmask) : 0.0f;
+  const uint32_t step = nsub * U;
+  for (uint32_t b0 = 0; b0 < count; b0 += step) {
+    uint32_t idx[U], rid[U];
+    uint4 w[U][NP];
+    float2 mt[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      idx[u] = b0 + sg + u * nsub;
+      rid[u] = ids[idx[u] < count ? idx[u] : count - 1];
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const uint4* row = reinterpret_cast<const uint4*>(base + (size_t)rid[u] * row_bytes);
+#pragma unroll
+      for (int j = 0; j < NP; ++j) {
+        const uint32_t p = s + 8u * j;
+        w[u][j] = p < Sh::kPieces ? __ldg(row + p) : make_uint4(0u, 0u, 0u, 0u);
       }
+      mt[u] = __ldg(meta + rid[u]);
+    }
+    float acc[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) acc[u] = 0.0f;
+#pragma unroll
+    for (int j = 0; j < NP; ++j) {
+      const uint32_t p = s + 8u * j;
+      if (p >= Sh::kPieces) continue;
+#pragma unroll
+      for (int u = 0; u < U; ++u) acc[u] = piece_dot<MODE>(w[u][j], q + p * kPer, acc[u]);
+    }
+#pragma unroll
+    for (int o = 1; o < 8; o <<= 1) {
+#pragma unroll
+      for (int u = 0; u < U; ++u) acc[u] += __shfl_xor_sync(gmask, acc[u], o, 8);
+    }
+    if (s == 0) {
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        if (idx[u] < count) d[idx[u]] = lp_distance<METRIC>(acc[u], mt[u], qq);
     }
   }
 }
@@ -685,10 +836,13 @@ __device__ __forceinline__ void cta_score(const SearchParams& P, const State& S,
       d[i] = pq_distance(P.codes + (size_t)ids[i] * P.cstride, S.table, P.pq_chunks);
   } else {
     const unsigned gmask = 0xFFu << (8u * ((tid & 31u) >> 3));
-    if (MODE == kModeFP32)
+    if constexpr (MODE == kModeFP32) {
       score_fp<METRIC, DIM, 1>(P, S.q, ids, d, count, tid >> 3, NT / 8, tid & 7u, gmask);
-    else
+    } else if constexpr (DIM > 0) {
+      score_lp_wide<METRIC, MODE, DIM>(P, S.q, ids, d, count, tid >> 3, NT / 8, tid & 7u, gmask);
+    } else {
       score_lp<METRIC, MODE, 1>(P, S.q, ids, d, count, tid >> 3, NT / 8, tid & 7u, gmask);
+    }
   }
 }
 
@@ -922,10 +1076,11 @@ __global__ void __launch_bounds__(NT) k_search_spill(const SearchParams P) {
 // Order key of a scored candidate at position i: distance ascending (an order-preserving
 // integer image of the float), then position descending (the later insert goes first);
 // NaN and padding sort after every valid key.
-__device__ __forceinline__ uint64_t new_item_key(const float* d, uint32_t i, uint32_t count) {
+__device__ __forceinline__ uint64_t new_item_key(const float* d, uint32_t i, uint32_t count,
+                                                 float tail) {
   if (i >= count) return ~0ull;
   const float x = d[i];
-  if (x != x) return ~0ull - 1u;
+  if (x != x || x > tail) return ~0ull - 1u;
   uint32_t u = __float_as_uint(x);
   u = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
   return ((uint64_t)u << 32) | (uint32_t)~i;
@@ -937,48 +1092,93 @@ __device__ __forceinline__ uint64_t shfl_xor64(uint64_t v, uint32_t m) {
   return ((uint64_t)hi << 32) | lo;
 }
 
+// Bitonic sort, ascending, of one 64-bit key per lane.
+__device__ __forceinline__ uint64_t warp_sort32(uint64_t k, uint32_t lane) {
+#pragma unroll
+  for (uint32_t size = 2; size <= 32u; size <<= 1) {
+#pragma unroll
+    for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+      const bool lower = (lane & stride) == 0u;
+      const bool asc = size == 32u || (lane & size) == 0u;
+      const uint64_t o = shfl_xor64(k, stride);
+      k = (lower == asc) ? min(k, o) : max(k, o);
+    }
+  }
+  return k;
+}
+
 // Sort the hop's scored candidates into new_{d,id}[0..nvalid) by (distance ascending,
 // position descending) — the order the reference's one-by-one inserts produce among
-// themselves.  Up to 64 items: a bitonic network over two keys per lane; beyond that a
-// counting rank.  Returns nvalid (NaN distances are dropped).
-__device__ __forceinline__ uint32_t warp_order_new(const State& S, uint32_t count, uint32_t lane) {
+// themselves.  Items that cannot enter the queue are dropped first: NaN distances, and,
+// when the queue is full, distances above its last entry `tail` (every queue entry precedes
+// them, so the merged top L+F is unchanged).  Up to 64 items: a bitonic network over one key
+// per lane when at most 32 remain, else two; beyond 64 a counting rank.  Returns nvalid.
+__device__ __forceinline__ uint32_t warp_order_new(const State& S, uint32_t count, uint32_t lane,
+                                                   float tail) {
   uint32_t nvalid = 0;
   if (count <= 64u) {
-    uint64_t k0 = new_item_key(S.cand_d, lane, count);
-    uint64_t k1 = new_item_key(S.cand_d, lane + 32u, count);
-    for (uint32_t size = 2; size <= 64u; size <<= 1) {
-      for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
-        if (stride == 32u) {  // index lane vs index lane+32, both in this lane; ascending
-          const uint64_t a = min(k0, k1), b = max(k0, k1);
-          k0 = a;
-          k1 = b;
-        } else {
-          const bool lower = (lane & stride) == 0u;
-          const bool asc0 = size == 64u || (lane & size) == 0u;
-          const bool asc1 = size == 64u || ((lane + 32u) & size) == 0u;
-          const uint64_t o0 = shfl_xor64(k0, stride), o1 = shfl_xor64(k1, stride);
-          k0 = (lower == asc0) ? min(k0, o0) : max(k0, o0);
-          k1 = (lower == asc1) ? min(k1, o1) : max(k1, o1);
+    uint64_t k0 = new_item_key(S.cand_d, lane, count, tail);
+    uint64_t k1 = new_item_key(S.cand_d, lane + 32u, count, tail);
+    const bool v0 = k0 < ~0ull - 1u, v1 = k1 < ~0ull - 1u;
+    const uint32_t m0 = __ballot_sync(kFull, v0), m1 = __ballot_sync(kFull, v1);
+    nvalid = __popc(m0) + __popc(m1);
+    if (nvalid == 0u) {
+      // nothing to place
+    } else if (nvalid <= 32u) {
+      // Compact the kept keys to one per lane (through new_d / new_id as scratch), sort 32.
+      uint32_t* hi = reinterpret_cast<uint32_t*>(S.new_d);
+      if (v0) {
+        const uint32_t r = __popc(m0 & lanemask_lt());
+        hi[r] = (uint32_t)(k0 >> 32);
+        S.new_id[r] = (uint32_t)k0;
+      }
+      if (v1) {
+        const uint32_t r = __popc(m0) + __popc(m1 & lanemask_lt());
+        hi[r] = (uint32_t)(k1 >> 32);
+        S.new_id[r] = (uint32_t)k1;
+      }
+      __syncwarp();
+      uint64_t k = lane < nvalid ? (((uint64_t)hi[lane] << 32) | S.new_id[lane]) : ~0ull;
+      __syncwarp();
+      k = warp_sort32(k, lane);
+      if (lane < nvalid) {
+        const uint32_t i = ~(uint32_t)k;
+        S.new_d[lane] = S.cand_d[i];
+        S.new_id[lane] = S.cand_id[i];
+      }
+    } else {
+      for (uint32_t size = 2; size <= 64u; size <<= 1) {
+        for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+          if (stride == 32u) {  // index lane vs index lane+32, both in this lane; ascending
+            const uint64_t a = min(k0, k1), b = max(k0, k1);
+            k0 = a;
+            k1 = b;
+          } else {
+            const bool lower = (lane & stride) == 0u;
+            const bool asc0 = size == 64u || (lane & size) == 0u;
+            const bool asc1 = size == 64u || ((lane + 32u) & size) == 0u;
+            const uint64_t o0 = shfl_xor64(k0, stride), o1 = shfl_xor64(k1, stride);
+            k0 = (lower == asc0) ? min(k0, o0) : max(k0, o0);
+            k1 = (lower == asc1) ? min(k1, o1) : max(k1, o1);
+          }
         }
       }
-    }
-    const bool v0 = k0 < ~0ull - 1u, v1 = k1 < ~0ull - 1u;
-    nvalid = __popc(__ballot_sync(kFull, v0)) + __popc(__ballot_sync(kFull, v1));
-    if (v0) {
-      const uint32_t i = ~(uint32_t)k0;
-      S.new_d[lane] = S.cand_d[i];
-      S.new_id[lane] = S.cand_id[i];
-    }
-    if (v1) {
-      const uint32_t i = ~(uint32_t)k1;
-      S.new_d[lane + 32u] = S.cand_d[i];
-      S.new_id[lane + 32u] = S.cand_id[i];
+      if (lane < nvalid) {
+        const uint32_t i = ~(uint32_t)k0;
+        S.new_d[lane] = S.cand_d[i];
+        S.new_id[lane] = S.cand_id[i];
+      }
+      if (lane + 32u < nvalid) {
+        const uint32_t i = ~(uint32_t)k1;
+        S.new_d[lane + 32u] = S.cand_d[i];
+        S.new_id[lane + 32u] = S.cand_id[i];
+      }
     }
   } else {
     for (uint32_t i0 = 0; i0 < count; i0 += 32u) {
       const uint32_t i = i0 + lane;
       const float d = i < count ? S.cand_d[i] : 0.0f;
-      const bool valid = i < count && d == d;
+      const bool valid = i < count && d == d && !(d > tail);
       if (valid) {
         uint32_t r = 0;
         for (uint32_t j = 0; j < count; ++j) {
@@ -993,6 +1193,12 @@ __device__ __forceinline__ uint32_t warp_order_new(const State& S, uint32_t coun
   }
   __syncwarp();
   return nvalid;
+}
+
+// Last entry of a full queue (items above it cannot enter), else +infinity.
+__device__ __forceinline__ float queue_tail(uint32_t cap, const State& S, uint32_t size,
+                                            uint32_t cur) {
+  return size == cap ? S.qd[cur][size - 1u] : INFINITY;
 }
 
 // Position of the first unvisited entry after merging the ordered new items (the next node
@@ -1017,6 +1223,7 @@ __device__ __forceinline__ uint32_t warp_next_cursor(uint32_t cap, const State& 
 }
 
 // Write the merged queue into the other buffer (see the file comment for the order rule).
+// Entries before the first insertion point p0 keep their positions; only the rest are ranked.
 __device__ __forceinline__ void warp_commit_merge(uint32_t cap, const State& S,
                                                   uint32_t nvalid, uint32_t nc, uint32_t lane,
                                                   uint32_t& size, uint32_t& cursor,
@@ -1027,14 +1234,19 @@ __device__ __forceinline__ void warp_commit_merge(uint32_t cap, const State& S,
   const uint32_t* oi = S.qi[cur];
   float* wd = S.qd[nxt];
   uint32_t* wi = S.qi[nxt];
-  for (uint32_t o = lane; o < size; o += 32u) {
+  const uint32_t p0 = nvalid ? count_less(od, size, S.new_d[0]) : size;
+  for (uint32_t o = lane; o < p0; o += 32u) {
+    wd[o] = od[o];
+    wi[o] = oi[o];
+  }
+  for (uint32_t o = p0 + lane; o < size; o += 32u) {
     const float d = od[o];
     const uint32_t pos = o + count_less_equal(S.new_d, nvalid, d);
     if (pos < cap) { wd[pos] = d; wi[pos] = oi[o]; }
   }
   for (uint32_t r = lane; r < nvalid; r += 32u) {
     const float d = S.new_d[r];
-    const uint32_t pos = r + count_less(od, size, d);
+    const uint32_t pos = r + p0 + count_less(od + p0, size - p0, d);
     if (pos < cap) { wd[pos] = d; wi[pos] = S.new_id[r]; }
   }
   cursor = nc;
@@ -1046,7 +1258,7 @@ __device__ __forceinline__ void warp_commit_merge(uint32_t cap, const State& S,
 __device__ __forceinline__ void warp_merge(uint32_t cap, const State& S, uint32_t count,
                                            uint32_t lane, uint32_t& size, uint32_t& cursor,
                                            uint32_t& cur) {
-  const uint32_t nvalid = warp_order_new(S, count, lane);
+  const uint32_t nvalid = warp_order_new(S, count, lane, queue_tail(cap, S, size, cur));
   uint32_t next_id;
   const uint32_t nc = warp_next_cursor(cap, S, nvalid, size, cursor, cur, next_id);
   warp_commit_merge(cap, S, nvalid, nc, lane, size, cursor, cur);
@@ -1071,10 +1283,13 @@ __device__ __forceinline__ void warp_score(const SearchParams& P, const State& S
       d[i] = pq_distance(P.codes + (size_t)ids[i] * P.cstride, S.table, P.pq_chunks);
   } else {
     const unsigned gmask = 0xFFu << (8u * (lane >> 3));
-    if (MODE == kModeFP32)
+    if constexpr (MODE == kModeFP32) {
       score_fp<METRIC, DIM, U>(P, S.q, ids, d, count, lane >> 3, 4u, lane & 7u, gmask);
-    else
+    } else if constexpr (DIM > 0) {
+      score_lp_wide<METRIC, MODE, DIM>(P, S.q, ids, d, count, lane >> 3, 4u, lane & 7u, gmask);
+    } else {
       score_lp<METRIC, MODE, 2>(P, S.q, ids, d, count, lane >> 3, 4u, lane & 7u, gmask);
+    }
   }
   __syncwarp();
 }
@@ -1214,24 +1429,36 @@ __device__ __forceinline__ void warp_query(const SearchParams& P, const State& S
           ids[r] = t < P.max_degree ? __ldg(row + 1 + t) : 0u;
         }
       }
-      for (uint32_t t0 = 0; t0 < deg; t0 += 32u) {
-        const uint32_t t = t0 + lane;
-        uint32_t id;
-        if (t0 < 128u) {
-          const uint32_t r = t0 >> 5;
-          id = r == 0 ? ids[0] : r == 1 ? ids[1] : r == 2 ? ids[2] : ids[3];
-        } else {
-          id = t < deg ? __ldg(row + 1 + t) : 0u;
+      if (deg <= 128u) {
+        bool fresh[4];
+        vset.insert_row(ids, deg, lane, fresh);
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          if (32u * r >= deg) break;
+          const uint32_t m = __ballot_sync(kFull, fresh[r]);
+          if (fresh[r]) S.cand_id[count + __popc(m & lanemask_lt())] = ids[r];
+          count += __popc(m);
         }
-        const bool fresh = vset.insert(t < deg, id);
-        const uint32_t m = __ballot_sync(kFull, fresh);
-        if (fresh) S.cand_id[count + __popc(m & lanemask_lt())] = id;
-        count += __popc(m);
+      } else {
+        for (uint32_t t0 = 0; t0 < deg; t0 += 32u) {
+          const uint32_t t = t0 + lane;
+          uint32_t id;
+          if (t0 < 128u) {
+            const uint32_t r = t0 >> 5;
+            id = r == 0 ? ids[0] : r == 1 ? ids[1] : r == 2 ? ids[2] : ids[3];
+          } else {
+            id = t < deg ? __ldg(row + 1 + t) : 0u;
+          }
+          const bool fresh = vset.insert(t < deg, id);
+          const uint32_t m = __ballot_sync(kFull, fresh);
+          if (fresh) S.cand_id[count + __popc(m & lanemask_lt())] = id;
+          count += __popc(m);
+        }
       }
     }
     __syncwarp();
     warp_score<METRIC, MODE, DIM, U>(P, S, S.cand_id, S.cand_d, count, lane);
-    const uint32_t nvalid = warp_order_new(S, count, lane);
+    const uint32_t nvalid = warp_order_new(S, count, lane, queue_tail(cap, S, size, cur));
     uint32_t next_id;
     const uint32_t nc = warp_next_cursor(cap, S, nvalid, size, cursor, cur, next_id);
     pf_node = P.beam == 1 ? next_id : kEmpty;

@@ -79,7 +79,8 @@ void base_params(const dk_index* ix, int32_t strategy, uint32_t k, uint32_t l, u
   P.offsets = ix->offsets;
   P.vec_bf16 = ix->vec_bf16;
   P.vec_fp8 = ix->vec_fp8;
-  P.fp8_scale = ix->fp8_scale;
+  P.bf16_meta = ix->bf16_meta;
+  P.fp8_meta = ix->fp8_meta;
   P.lp_stride = ix->lp_stride;
   P.n = ix->n;
   P.f = ix->f;
@@ -129,7 +130,7 @@ int32_t plan_warp(dk_index* ix, SearchParams& P, LaunchPlan& L, int mode, double
   // shared-memory budget; the global level takes what a longer search adds.
   P.hash_log2 = 0;
   const uint32_t base = plan_query_smem(P, pq, false);
-  const uint32_t budget = std::max<uint32_t>(env_u32("DK_WARP_SMEM", 24576), base + 1024);
+  const uint32_t budget = std::max<uint32_t>(env_u32("DK_WARP_SMEM", 12288), base + 1024);
   uint32_t slots = align_up((uint32_t)(est_mean * 1.3 / 0.75) + 1, 32);
   slots = std::min<uint32_t>(slots, ((budget - base) / 4) & ~31u);
   if (const uint32_t hl = env_u32("DK_HASH_LOG2", 0)) slots = 1u << std::min<uint32_t>(hl, 16);
@@ -141,9 +142,12 @@ int32_t plan_warp(dk_index* ix, SearchParams& P, LaunchPlan& L, int mode, double
   plan_query_smem(P, pq, false);
   P.off_hash = base;
   if (P.warp_smem > (uint32_t)max_optin) return too_big();
-  P.gtable_log2 = log2_at_least(std::max(est, 2.0 * P.hash_limit) / 0.75, 10, 22);
+  // Global level: open addressing probed one CAS per step, so its load stays low (a warp waits
+  // for the longest of its 32 lanes' probe chains).  DK_GTABLE_LOAD (percent) overrides.
+  const double gload = std::min(0.75, std::max(0.05, env_u32("DK_GTABLE_LOAD", 75) / 100.0));
+  P.gtable_log2 = log2_at_least(std::max(est, 2.0 * P.hash_limit) / gload, 10, 22);
   P.gtable_log2 = std::min<uint32_t>(std::max<uint32_t>(env_u32("DK_GTABLE_LOG2", P.gtable_log2), 6), 24);
-  P.gtable_limit = (uint32_t)((1u << P.gtable_log2) * 0.75);
+  P.gtable_limit = (uint32_t)((1u << P.gtable_log2) * gload);
   // Warps per CTA: the packing with the most resident warps per SM.
   int best_warps = 0;
   for (uint32_t wpc : {4u, 2u, 1u}) {
