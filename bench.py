@@ -259,11 +259,22 @@ def serve_latency(provider, strategy, queries, k, l, rate, seconds, seed=1):
     elapsed = time.perf_counter() - t0
     info = srv.info()
     srv.close()
-    lat = np.sort(lat[:done])
-    pick = lambda p: float(lat[min(int(p * len(lat) / 100), len(lat) - 1)]) * 1e3
+    pct = percentiles(lat[:done] * 1e3)
     return {"offered_qps": rate, "achieved_qps": round(done / elapsed, 1), "requests": done,
-            "p50_ms": round(pick(50), 4), "p99_ms": round(pick(99), 4),
+            "p50_ms": round(pct["median"], 4), "p90_ms": round(pct["p90"], 4),
+            "p99_ms": round(pct["p99"], 4), "mean_ms": round(pct["mean"], 4),
             "launches": int(info["launches"]), "streams": int(info["streams"])}
+
+
+def percentiles(x):
+    """The benchmark runner's rule (diskann-benchmark-runner/src/utils/percentiles.rs:59-85):
+    sorted; median = middle element or the mean of the two middle ones; p90 = x[min(9n/10,
+    n-1)]; p99 = x[min(99n/100, n-1)]."""
+    x = np.sort(np.asarray(x, dtype=np.float64))
+    n = len(x)
+    med = x[n // 2] if n % 2 == 1 else (x[n // 2 - 1] + x[n // 2]) / 2.0
+    return {"mean": float(x.mean()), "median": float(med), "p90": float(x[min(9 * n // 10, n - 1)]),
+            "p99": float(x[min(99 * n // 100, n - 1)])}
 
 
 def run_ours(args, data, rank, world):
@@ -453,6 +464,17 @@ def cpu_baseline(data, strategy, l, threads, min_seconds=2.0, max_reps=5, nq=Non
     return total / el, reps, res
 
 
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown CPU"
+
+
 def barrier(world):
     if world > 1:
         import torch.distributed as dist
@@ -573,7 +595,8 @@ def main():
                 "cpu_baseline": {"value": round(value, 1), "unit": "queries/s", "cores": threads,
                                  "kind": "port",
                                  "sample": f"{sample} of the {w['nq']} queries per step, "
-                                           f"{threads} threads, FullPrecision L={l}"},
+                                           f"{threads} threads, FullPrecision L={l}, "
+                                           f"{cpu_model()}"},
                 "e2e": {"value": round(value, 1), "unit": "queries/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
@@ -599,7 +622,7 @@ def main():
             qps, reps, _ = cpu_baseline(data, cpu_strat, cpu_l, threads, nq=sample)
             cpu = {"value": round(qps, 1), "unit": "queries/s", "cores": threads, "kind": "port",
                    "sample": f"{reps} x {sample} queries, {threads} threads, "
-                             f"{cpu_strat} L={cpu_l}"}
+                             f"{cpu_strat} L={cpu_l}, {cpu_model()}"}
         line = {
             "metric": METRIC_NAME, "value": round(r["value"], 1), "unit": "queries/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,

@@ -73,19 +73,28 @@ struct SmemHashSet {
     for (uint32_t i = tid; i <= mask; i += nt) slots[i] = kEmpty;
   }
   // True if `id` was absent (and is now present).  Callers keep the load at most 3/4, so
-  // the probe always ends.
+  // the probe always ends.  Linear probing over 16-byte buckets of four slots, one shared
+  // read per bucket; slots fill in probe order and are never removed, so the first empty slot
+  // ends a lookup.  Threads may insert the same id at once: a lost CAS re-reads the bucket.
   __device__ bool insert(uint32_t id) const {
-    volatile uint32_t* s = slots;
-    uint32_t h = (id * 2654435761u) >> shift;
+    const uint32_t base = (uint32_t)__cvta_generic_to_shared(slots);
+    const uint32_t bmask = mask >> 2;
+    uint32_t b = ((id * 2654435761u) >> shift) >> 2;
     while (true) {
-      const uint32_t cur = s[h];
-      if (cur == id) return false;
-      if (cur == kEmpty) {
-        const uint32_t old = atomicCAS(&slots[h], kEmpty, id);
+      uint32_t v[4];
+      asm volatile("ld.volatile.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
+                   : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3])
+                   : "r"(base + 16u * b));
+      if (v[0] == id || v[1] == id || v[2] == id || v[3] == id) return false;
+      const uint32_t j = v[0] == kEmpty ? 0u : v[1] == kEmpty ? 1u : v[2] == kEmpty ? 2u
+                                                              : v[3] == kEmpty ? 3u : 4u;
+      if (j < 4u) {
+        const uint32_t old = atomicCAS(&slots[4u * b + j], kEmpty, id);
         if (old == kEmpty) return true;
         if (old == id) return false;
+        continue;  // another id took the slot: read the bucket again
       }
-      h = (h + 1) & mask;
+      b = (b + 1u) & bmask;
     }
   }
 };
@@ -851,9 +860,11 @@ __device__ __forceinline__ void cta_merge(const SearchParams& P, const State& S,
   const uint32_t tid = threadIdx.x;
   Misc* M = S.misc;
   uint32_t my_valid = 0;
+  // Items that cannot enter are dropped: NaN, and above the last entry of a full queue.
+  const float tail = M->size == P.cap ? S.qd[M->cur][M->size - 1u] : INFINITY;
   for (uint32_t i = tid; i < count; i += NT) {
     const float d = S.cand_d[i];
-    if (d != d) continue;
+    if (d != d || d > tail) continue;
     uint32_t r = 0;
     for (uint32_t j = 0; j < count; ++j) {
       const float dj = S.cand_d[j];
@@ -873,14 +884,20 @@ __device__ __forceinline__ void cta_merge(const SearchParams& P, const State& S,
   const uint32_t* oi = S.qi[cur];
   float* wd = S.qd[nxt];
   uint32_t* wi = S.qi[nxt];
-  for (uint32_t o = tid; o < size; o += NT) {
+  // Entries before the first insertion point keep their positions; the rest are ranked.
+  const uint32_t p0 = nvalid ? count_less(od, size, S.new_d[0]) : size;
+  for (uint32_t o = tid; o < p0; o += NT) {
+    wd[o] = od[o];
+    wi[o] = oi[o];
+  }
+  for (uint32_t o = p0 + tid; o < size; o += NT) {
     const float d = od[o];
     const uint32_t pos = o + count_less_equal(S.new_d, nvalid, d);
     if (pos < cap) { wd[pos] = d; wi[pos] = oi[o]; }
   }
   for (uint32_t r = tid; r < nvalid; r += NT) {
     const float d = S.new_d[r];
-    const uint32_t pos = r + count_less(od, size, d);
+    const uint32_t pos = r + p0 + count_less(od + p0, size - p0, d);
     if (pos < cap) { wd[pos] = d; wi[pos] = S.new_id[r]; }
   }
   __syncthreads();
@@ -1264,6 +1281,29 @@ __device__ __forceinline__ void warp_merge(uint32_t cap, const State& S, uint32_
   warp_commit_merge(cap, S, nvalid, nc, lane, size, cursor, cur);
 }
 
+// Ask L2 for the scored rows of every neighbour in a row (up to 128) while the visited filter
+// runs, so the scoring that follows finds them in L2.  Visited neighbours are fetched too:
+// extra traffic traded for a shorter dependent chain per hop.
+template <int MODE>
+__device__ __forceinline__ void prefetch_rows(const SearchParams& P, const uint32_t (&ids)[4],
+                                              uint32_t deg, uint32_t lane) {
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const uint32_t t = 32u * r + lane;
+    if (t >= deg || t >= 128u) continue;
+    const uint32_t id = ids[r];
+    if (MODE == kModeFP32) {
+      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;"
+                   :: "l"(P.vectors + (size_t)id * P.vstride), "r"(P.vstride * 4u) : "memory");
+    } else if (MODE == kModeBF16 || MODE == kModeFP8) {
+      const unsigned char* row = lp_rows<MODE>(P) + (size_t)id * P.lp_stride * (MODE == kModeBF16 ? 2u : 1u);
+      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;"
+                   :: "l"(row), "r"(P.lp_stride * (MODE == kModeBF16 ? 2u : 1u)) : "memory");
+      asm volatile("prefetch.global.L2 [%0];" :: "l"(lp_meta<MODE>(P) + id) : "memory");
+    }
+  }
+}
+
 // One query's inputs and outputs (a batch row, or a serving request).
 struct QueryIO {
   const float* query;
@@ -1429,7 +1469,10 @@ __device__ __forceinline__ void warp_query(const SearchParams& P, const State& S
           ids[r] = t < P.max_degree ? __ldg(row + 1 + t) : 0u;
         }
       }
-      if (deg <= 128u) {
+      if (P.prefetch) prefetch_rows<MODE>(P, ids, deg, lane);
+      // Low-precision traversal: a row's global-level probes go out together.  The FP32 path
+      // keeps one round at a time, which measured faster with its register-heavier scoring.
+      if ((MODE == kModeBF16 || MODE == kModeFP8) && deg <= 128u) {
         bool fresh[4];
         vset.insert_row(ids, deg, lane, fresh);
 #pragma unroll
