@@ -59,24 +59,24 @@ inline float simd_order(const float* x, const float* y, size_t len) {
   return (q0 + q2) + (q1 + q3);
 }
 
+// CosineStateless on x86-64-v3: Strategy2x4 (simd.rs:422-482) — full 8-wide vectors
+// alternate between two accumulator sets, combined as set0 + set1, then the masked remainder.
 float cosine_sim(const float* x, const float* y, size_t len) {
-  float sx[4][8] = {}, sy[4][8] = {}, sxy[4][8] = {};
-  const size_t trip = len / 32, epi = (len - 32 * trip) / 8;
-  auto step = [&](int j, int l, size_t e) {
-    sx[j][l] = std::fma(x[e], x[e], sx[j][l]);
-    sy[j][l] = std::fma(y[e], y[e], sy[j][l]);
-    sxy[j][l] = std::fma(x[e], y[e], sxy[j][l]);
-  };
-  for (size_t b = 0; b < trip; ++b)
-    for (int j = 0; j < 4; ++j)
-      for (int l = 0; l < 8; ++l) step(j, l, 32 * b + 8 * j + l);
-  for (size_t j = 0; j < epi; ++j)
-    for (int l = 0; l < 8; ++l) step((int)j, l, 32 * trip + 8 * j + l);
+  float sx[2][8] = {}, sy[2][8] = {}, sxy[2][8] = {};
+  const size_t nvec = len / 8;
+  for (size_t k = 0; k < nvec; ++k)
+    for (int l = 0; l < 8; ++l) {
+      const size_t e = 8 * k + l;
+      const int j = (int)(k & 1);
+      sx[j][l] = std::fma(x[e], x[e], sx[j][l]);
+      sy[j][l] = std::fma(y[e], y[e], sy[j][l]);
+      sxy[j][l] = std::fma(x[e], y[e], sxy[j][l]);
+    }
   float tx[8], ty[8], txy[8];
   for (int l = 0; l < 8; ++l) {
-    tx[l] = (sx[0][l] + sx[1][l]) + (sx[2][l] + sx[3][l]);
-    ty[l] = (sy[0][l] + sy[1][l]) + (sy[2][l] + sy[3][l]);
-    txy[l] = (sxy[0][l] + sxy[1][l]) + (sxy[2][l] + sxy[3][l]);
+    tx[l] = sx[0][l] + sx[1][l];
+    ty[l] = sy[0][l] + sy[1][l];
+    txy[l] = sxy[0][l] + sxy[1][l];
   }
   const size_t rem = len % 8, base = len - rem;
   for (size_t l = 0; l < rem; ++l) {

@@ -90,7 +90,6 @@ struct SearchParams {
   uint32_t smem_bytes;
   uint32_t warp_smem;
   uint32_t list_cap;  // capacity of the candidate / rerank lists
-  uint32_t prefetch;  // warp kernel: L2-prefetch every neighbour's scored row before filtering
   uint32_t* hint;     // device words of the visited-size hint (may be null)
   // Serving launches: per-request (k, L) pairs; outputs keep a stride of `k` (= max_k).
   // Null for batch launches, where every query uses `k` and `l`.

@@ -380,69 +380,55 @@ __device__ __forceinline__ void subgroup_distances(const float* const (&rows)[U]
   }
 }
 
-// Cosine (CosineStateless, simd.rs:2430-2460): three accumulators with the same lane
-// mapping; sum (simd.rs:2327-2361): zero similarity if a norm is below f32::MIN_POSITIVE,
-// else clamp(prod / (sqrt(nx) * sqrt(ny)), -1, 1); distance 1 - similarity.
+// Cosine (CosineStateless, simd.rs:2430-2460) on x86-64-v3 runs Strategy2x4
+// (simd.rs:422-482): three accumulators (x*x, y*y, x*y) in two sets, full 8-wide vectors in
+// order alternating between the sets (vector k -> set k % 2), combined as set0 + set1, then a
+// masked remainder.  Lane s of the subgroup is SIMD lane s: it runs both sets' FMA chains for
+// element 8k + s.  sum (simd.rs:2327-2361): sum_tree of each accumulator (xor 4, 2, 1 over the
+// 8 lanes gives (t_i + t_{i+4}), then (q0 + q2) + (q1 + q3)); zero similarity if a norm is
+// below f32::MIN_POSITIVE, else clamp(prod / (sqrt(nx) * sqrt(ny))); distance 1 - similarity.
 template <int DIM>
 __device__ __forceinline__ float subgroup_cosine(const float* __restrict__ row,
                                                  const float* __restrict__ q, uint32_t dim_rt,
                                                  uint32_t s, unsigned gmask) {
   const uint32_t dim = DIM > 0 ? (uint32_t)DIM : dim_rt;
-  const uint32_t rem = dim & 7u;
-  const uint32_t full = dim - rem;
-  const float4* row4 = reinterpret_cast<const float4*>(row);
-  const float4* q4 = reinterpret_cast<const float4*>(q);
-  float xx[4] = {0.f, 0.f, 0.f, 0.f}, yy[4] = {0.f, 0.f, 0.f, 0.f}, xy[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll 4
-  for (uint32_t base = 4u * s; base < full; base += 32u) {
-    const float4 v = __ldg(row4 + (base >> 2));
-    const float4 a = q4[base >> 2];
-    const float av[4] = {a.x, a.y, a.z, a.w}, vv[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      xx[i] = __fmaf_rn(av[i], av[i], xx[i]);
-      yy[i] = __fmaf_rn(vv[i], vv[i], yy[i]);
-      xy[i] = __fmaf_rn(av[i], vv[i], xy[i]);
-    }
+  const uint32_t nvec = dim >> 3;
+  float x0 = 0.f, y0 = 0.f, p0 = 0.f, x1 = 0.f, y1 = 0.f, p1 = 0.f;
+  uint32_t k = 0;
+#pragma unroll 8
+  for (; k + 1u < nvec; k += 2u) {
+    const float b0 = __ldg(row + 8u * k + s), b1 = __ldg(row + 8u * k + 8u + s);
+    const float a0 = q[8u * k + s], a1 = q[8u * k + 8u + s];
+    x0 = __fmaf_rn(a0, a0, x0);
+    y0 = __fmaf_rn(b0, b0, y0);
+    p0 = __fmaf_rn(a0, b0, p0);
+    x1 = __fmaf_rn(a1, a1, x1);
+    y1 = __fmaf_rn(b1, b1, y1);
+    p1 = __fmaf_rn(a1, b1, p1);
+  }
+  if (k < nvec) {
+    const float b0 = __ldg(row + 8u * k + s), a0 = q[8u * k + s];
+    x0 = __fmaf_rn(a0, a0, x0);
+    y0 = __fmaf_rn(b0, b0, y0);
+    p0 = __fmaf_rn(a0, b0, p0);
+  }
+  float tx = x0 + x1, ty = y0 + y1, tp = p0 + p1;
+  if (s < (dim & 7u)) {
+    const float b = __ldg(row + 8u * nvec + s), a = q[8u * nvec + s];
+    tx = __fmaf_rn(a, a, tx);
+    ty = __fmaf_rn(b, b, ty);
+    tp = __fmaf_rn(a, b, tp);
   }
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    xx[i] += __shfl_xor_sync(gmask, xx[i], 2, 8);
-    yy[i] += __shfl_xor_sync(gmask, yy[i], 2, 8);
-    xy[i] += __shfl_xor_sync(gmask, xy[i], 2, 8);
-    xx[i] += __shfl_xor_sync(gmask, xx[i], 4, 8);
-    yy[i] += __shfl_xor_sync(gmask, yy[i], 4, 8);
-    xy[i] += __shfl_xor_sync(gmask, xy[i], 4, 8);
+  for (int o = 4; o > 0; o >>= 1) {
+    tx += __shfl_xor_sync(gmask, tx, o, 8);
+    ty += __shfl_xor_sync(gmask, ty, o, 8);
+    tp += __shfl_xor_sync(gmask, tp, o, 8);
   }
-  if (rem) {
-    const uint32_t e = full + 4u * (s & 1u);
-    if (e < dim) {
-      const float4 v = __ldg(row4 + (e >> 2));
-      const float4 a = q4[e >> 2];
-      const float av[4] = {a.x, a.y, a.z, a.w}, vv[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        if (e + i < dim) {
-          xx[i] = __fmaf_rn(av[i], av[i], xx[i]);
-          yy[i] = __fmaf_rn(vv[i], vv[i], yy[i]);
-          xy[i] = __fmaf_rn(av[i], vv[i], xy[i]);
-        }
-      }
-    }
-  }
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    xx[i] += __shfl_xor_sync(gmask, xx[i], 1, 8);
-    yy[i] += __shfl_xor_sync(gmask, yy[i], 1, 8);
-    xy[i] += __shfl_xor_sync(gmask, xy[i], 1, 8);
-  }
-  const float nx = tree4(xx[0], xx[1], xx[2], xx[3]);
-  const float ny = tree4(yy[0], yy[1], yy[2], yy[3]);
-  const float denom = __fmul_rn(__fsqrt_rn(nx), __fsqrt_rn(ny));
-  const float prod = tree4(xy[0], xy[1], xy[2], xy[3]);
+  const float denom = __fmul_rn(__fsqrt_rn(tx), __fsqrt_rn(ty));
   float sim;
-  if (nx < 1.17549435e-38f || ny < 1.17549435e-38f) sim = 0.0f;
-  else sim = fmaxf(-1.0f, fminf(1.0f, __fdiv_rn(prod, denom)));
+  if (tx < 1.17549435e-38f || ty < 1.17549435e-38f) sim = 0.0f;
+  else sim = fmaxf(-1.0f, fminf(1.0f, __fdiv_rn(tp, denom)));
   return 1.0f - sim;
 }
 
@@ -1281,29 +1267,6 @@ __device__ __forceinline__ void warp_merge(uint32_t cap, const State& S, uint32_
   warp_commit_merge(cap, S, nvalid, nc, lane, size, cursor, cur);
 }
 
-// Ask L2 for the scored rows of every neighbour in a row (up to 128) while the visited filter
-// runs, so the scoring that follows finds them in L2.  Visited neighbours are fetched too:
-// extra traffic traded for a shorter dependent chain per hop.
-template <int MODE>
-__device__ __forceinline__ void prefetch_rows(const SearchParams& P, const uint32_t (&ids)[4],
-                                              uint32_t deg, uint32_t lane) {
-#pragma unroll
-  for (int r = 0; r < 4; ++r) {
-    const uint32_t t = 32u * r + lane;
-    if (t >= deg || t >= 128u) continue;
-    const uint32_t id = ids[r];
-    if (MODE == kModeFP32) {
-      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;"
-                   :: "l"(P.vectors + (size_t)id * P.vstride), "r"(P.vstride * 4u) : "memory");
-    } else if (MODE == kModeBF16 || MODE == kModeFP8) {
-      const unsigned char* row = lp_rows<MODE>(P) + (size_t)id * P.lp_stride * (MODE == kModeBF16 ? 2u : 1u);
-      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;"
-                   :: "l"(row), "r"(P.lp_stride * (MODE == kModeBF16 ? 2u : 1u)) : "memory");
-      asm volatile("prefetch.global.L2 [%0];" :: "l"(lp_meta<MODE>(P) + id) : "memory");
-    }
-  }
-}
-
 // One query's inputs and outputs (a batch row, or a serving request).
 struct QueryIO {
   const float* query;
@@ -1469,7 +1432,6 @@ __device__ __forceinline__ void warp_query(const SearchParams& P, const State& S
           ids[r] = t < P.max_degree ? __ldg(row + 1 + t) : 0u;
         }
       }
-      if (P.prefetch) prefetch_rows<MODE>(P, ids, deg, lane);
       // Low-precision traversal: a row's global-level probes go out together.  The FP32 path
       // keeps one round at a time, which measured faster with its register-heavier scoring.
       if ((MODE == kModeBF16 || MODE == kModeFP8) && deg <= 128u) {

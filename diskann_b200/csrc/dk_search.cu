@@ -96,7 +96,6 @@ void base_params(const dk_index* ix, int32_t strategy, uint32_t k, uint32_t l, u
   P.beam = beam;
   P.strategy = strategy;
   P.list_cap = std::max(std::max(beam * ix->max_degree, P.cap), ix->f);
-  P.prefetch = env_u32("DK_PREFETCH", 0);
 }
 
 void visited_estimates(dk_index* ix, const SearchParams& P, double& est, double& est_mean) {

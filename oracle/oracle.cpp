@@ -93,48 +93,61 @@ float simd_op_v3(const float* x, const float* y, size_t len) {
 }
 
 // Cosine: `CosineStateless` on x86-64-v3 (simd.rs:2430-2460) keeps three f32x8
-// accumulators (x*x, y*y, x*y; FullCosineAccumulator::add_with, simd.rs:2307-2315) with
-// `Strategy2x4` (simd.rs:424-470; BLOCK_SIZE 4 so element-to-accumulator mapping is the
-// same as Strategy4x1).  `sum` (simd.rs:2327-2361): norms and product via sum_tree, zero
-// if either norm is below f32::MIN_POSITIVE, otherwise clamp(prod / (sqrt(nx)*sqrt(ny))).
-float cosine_similarity_v3(const float* x, const float* y, size_t len) {
-  float sx[4][8], sy[4][8], sxy[4][8];
+// accumulators (x*x, y*y, x*y; FullCosineAccumulator::add_with, simd.rs:2307-2315) and runs
+// the `Strategy2x4` main loop (simd.rs:422-482): two accumulator sets, the full 8-wide vectors
+// in order alternating between them (vector k goes to set k % 2, the peeled odd block and the
+// 1-3 full-width epilogues continue the same alternation), combined as s0 + s1; a remainder
+// shorter than 8 is then masked-loaded into the combined set (simd.rs:686-745).  `sum`
+// (simd.rs:2327-2361): norms and product via sum_tree, zero similarity if either norm is below
+// f32::MIN_POSITIVE, otherwise clamp(prod / (sqrt(nx) * sqrt(ny)), -1, 1).
+struct CosAcc {
+  float x[8], y[8], xy[8];
+};
+
+// One `simd_op` of CosineStateless over a slice, before `sum`: the combined accumulator.
+CosAcc cosine_accumulate_v3(const float* x, const float* y, size_t len) {
+  float sx[2][8], sy[2][8], sxy[2][8];
   std::memset(sx, 0, sizeof(sx));
   std::memset(sy, 0, sizeof(sy));
   std::memset(sxy, 0, sizeof(sxy));
-  const size_t trip = len / 32;
-  const size_t epilogues = (len - 32 * trip) / 8;
-  auto step = [&](int j, int l, size_t e) {
-    sx[j][l] = std::fmaf(x[e], x[e], sx[j][l]);
-    sy[j][l] = std::fmaf(y[e], y[e], sy[j][l]);
-    sxy[j][l] = std::fmaf(x[e], y[e], sxy[j][l]);
-  };
-  for (size_t b = 0; b < trip; ++b)
-    for (int j = 0; j < 4; ++j)
-      for (int l = 0; l < 8; ++l) step(j, l, 32 * b + 8 * j + l);
-  for (size_t j = 0; j < epilogues; ++j)
-    for (int l = 0; l < 8; ++l) step((int)j, l, 32 * trip + 8 * j + l);
-  float tx[8], ty[8], txy[8];
+  const size_t nvec = len / 8;
+  for (size_t k = 0; k < nvec; ++k)
+    for (int l = 0; l < 8; ++l) {
+      const float a = x[8 * k + l], b = y[8 * k + l];
+      const int j = (int)(k & 1);
+      sx[j][l] = std::fmaf(a, a, sx[j][l]);
+      sy[j][l] = std::fmaf(b, b, sy[j][l]);
+      sxy[j][l] = std::fmaf(a, b, sxy[j][l]);
+    }
+  CosAcc t;
   for (int l = 0; l < 8; ++l) {
-    tx[l] = (sx[0][l] + sx[1][l]) + (sx[2][l] + sx[3][l]);
-    ty[l] = (sy[0][l] + sy[1][l]) + (sy[2][l] + sy[3][l]);
-    txy[l] = (sxy[0][l] + sxy[1][l]) + (sxy[2][l] + sxy[3][l]);
+    t.x[l] = sx[0][l] + sx[1][l];
+    t.y[l] = sy[0][l] + sy[1][l];
+    t.xy[l] = sxy[0][l] + sxy[1][l];
   }
   const size_t rem = len % 8;
   const size_t base = len - rem;
   for (size_t l = 0; l < rem; ++l) {
     const float a = x[base + l], b = y[base + l];
-    tx[l] = std::fmaf(a, a, tx[l]);
-    ty[l] = std::fmaf(b, b, ty[l]);
-    txy[l] = std::fmaf(a, b, txy[l]);
+    t.x[l] = std::fmaf(a, a, t.x[l]);
+    t.y[l] = std::fmaf(b, b, t.y[l]);
+    t.xy[l] = std::fmaf(a, b, t.xy[l]);
   }
-  const float nx = sum_tree8(tx);
-  const float ny = sum_tree8(ty);
+  return t;
+}
+
+float cosine_sum_v3(const CosAcc& t) {
+  const float nx = sum_tree8(t.x);
+  const float ny = sum_tree8(t.y);
   const float denom = std::sqrt(nx) * std::sqrt(ny);
-  const float prod = sum_tree8(txy);
+  const float prod = sum_tree8(t.xy);
   if (nx < 1.17549435e-38f || ny < 1.17549435e-38f) return 0.0f;
   const float v = prod / denom;
   return std::max(-1.0f, std::min(1.0f, v));
+}
+
+float cosine_similarity_v3(const float* x, const float* y, size_t len) {
+  return cosine_sum_v3(cosine_accumulate_v3(x, y, len));
 }
 
 }  // namespace

@@ -62,3 +62,21 @@ def test_pq_codes_roundtrip(tmp_path):
     p = tmp_path / "codes.bin"
     formats.write_pq_codes(str(p), codes)
     np.testing.assert_array_equal(formats.read_pq_codes(str(p)), codes)
+
+
+@pytest.mark.parametrize("metric", [0, 1, 2, 3])
+def test_host_distance_matches_oracle(metric):
+    """dk_distance (host tooling, C ABI) reproduces the oracle's rounding sequence bit for bit."""
+    from diskann_b200 import graph
+    from oracle import oracle as O
+
+    rng = np.random.default_rng(40 + metric)
+    for n in (1, 7, 8, 13, 16, 31, 32, 33, 96, 100, 128, 384):
+        x = rng.standard_normal(n).astype(np.float32)
+        y = rng.standard_normal(n).astype(np.float32)
+        if metric == 3:
+            x /= np.linalg.norm(x)
+            y /= np.linalg.norm(y)
+        got = np.float32(graph.distance(metric, x, y))
+        ref = np.float32(O.distance(metric, x, y))
+        assert got.view(np.uint32) == ref.view(np.uint32), (metric, n, got, ref)

@@ -109,3 +109,86 @@ def test_oracle_search_finds_exact_on_complete_graph():
     gt, _ = O.bruteforce_f64(base, q, 5, O.METRIC_L2)
     assert list(ids[0]) == list(gt[0])
     assert st[0]["cmps"] == n + 1
+
+
+# ---------------------------------------------------------------------------------------
+# The x86-64-v3 accumulation orders, restated independently in numpy (float32 rounding after
+# every operation; fma emulated in float64, exact for these inputs up to a double rounding
+# that is vanishingly rare), against the oracle's distance function bit for bit.
+# ---------------------------------------------------------------------------------------
+
+def _f32(x):
+    return np.float32(x)
+
+
+def _fma(a, b, c):
+    return np.float32(np.float64(a) * np.float64(b) + np.float64(c))
+
+
+def _sum_tree(t):
+    q = [_f32(t[i] + t[i + 4]) for i in range(4)]
+    return _f32(_f32(q[0] + q[2]) + _f32(q[1] + q[3]))
+
+
+def _strategy_4x1(x, y, l2):
+    """L2 / IP on V3: Strategy4x1 (simd.rs:321-363), then the masked remainder."""
+    n = len(x)
+    s = np.zeros((4, 8), np.float32)
+    trip, k = n // 32, 0
+    for k in range(trip * 4 + (n - 32 * trip) // 8):
+        j = k % 4 if k < 4 * trip else (k - 4 * trip)
+        for lane in range(8):
+            e = 8 * k + lane
+            c = _f32(x[e] - y[e]) if l2 else None
+            s[j][lane] = _fma(c, c, s[j][lane]) if l2 else _fma(x[e], y[e], s[j][lane])
+    t = [_f32(_f32(s[0][i] + s[1][i]) + _f32(s[2][i] + s[3][i])) for i in range(8)]
+    base = n - n % 8
+    for lane in range(n % 8):
+        e = base + lane
+        if l2:
+            c = _f32(x[e] - y[e])
+            t[lane] = _fma(c, c, t[lane])
+        else:
+            t[lane] = _fma(x[e], y[e], t[lane])
+    return _sum_tree(t)
+
+
+def _cosine_2x4(x, y):
+    """CosineStateless on V3: Strategy2x4 (simd.rs:422-482), masked remainder, then `sum`."""
+    n = len(x)
+    acc = np.zeros((3, 2, 8), np.float32)
+    for k in range(n // 8):
+        for lane in range(8):
+            a, b = x[8 * k + lane], y[8 * k + lane]
+            acc[0][k % 2][lane] = _fma(a, a, acc[0][k % 2][lane])
+            acc[1][k % 2][lane] = _fma(b, b, acc[1][k % 2][lane])
+            acc[2][k % 2][lane] = _fma(a, b, acc[2][k % 2][lane])
+    t = [[_f32(acc[q][0][i] + acc[q][1][i]) for i in range(8)] for q in range(3)]
+    base = n - n % 8
+    for lane in range(n % 8):
+        a, b = x[base + lane], y[base + lane]
+        t[0][lane] = _fma(a, a, t[0][lane])
+        t[1][lane] = _fma(b, b, t[1][lane])
+        t[2][lane] = _fma(a, b, t[2][lane])
+    nx, ny, xy = _sum_tree(t[0]), _sum_tree(t[1]), _sum_tree(t[2])
+    if nx < 1.17549435e-38 or ny < 1.17549435e-38:
+        sim = np.float32(0.0)
+    else:
+        den = _f32(_f32(np.sqrt(nx)) * _f32(np.sqrt(ny)))
+        sim = np.float32(max(-1.0, min(1.0, float(_f32(xy / den)))))
+    return _f32(np.float32(1.0) - sim)
+
+
+@pytest.mark.parametrize("n", [1, 5, 8, 13, 16, 24, 31, 32, 33, 40, 56, 96, 100, 128, 200, 384])
+def test_oracle_accumulation_orders(n):
+    rng = np.random.default_rng(n)
+    for trial in range(3):
+        scale = np.float32(10.0 ** rng.uniform(-2, 2))
+        x = (rng.standard_normal(n) * scale).astype(np.float32)
+        y = (rng.standard_normal(n) * scale).astype(np.float32)
+        got_l2 = np.float32(O.distance(O.METRIC_L2, x, y))
+        got_ip = np.float32(O.distance(O.METRIC_INNER_PRODUCT, x, y))
+        got_cos = np.float32(O.distance(O.METRIC_COSINE, x, y))
+        assert got_l2.view(np.uint32) == _strategy_4x1(x, y, True).view(np.uint32)
+        assert got_ip.view(np.uint32) == np.float32(-_strategy_4x1(x, y, False)).view(np.uint32)
+        assert got_cos.view(np.uint32) == _cosine_2x4(x, y).view(np.uint32)
