@@ -79,8 +79,6 @@ int32_t dk_check_search_args(const dk_index* ix, int32_t strategy, uint32_t k, u
     return fail(DK_ERR_INVALID_ARGUMENT, "unknown strategy");
   if (strategy == DK_STRATEGY_HYBRID || strategy == DK_STRATEGY_QUANTIZED) {
     if (ix->pq_chunks == 0) return fail(DK_ERR_NO_PQ, "index has no PQ data");
-    if (ix->metric == DK_METRIC_COSINE)
-      return fail(DK_ERR_UNSUPPORTED, "PQ traversal with the Cosine metric is not supported");
   }
   if (strategy == DK_STRATEGY_BF16 && !ix->vec_bf16)
     return fail(DK_ERR_NO_LOW_PRECISION, "index was created without DK_INDEX_BF16");

@@ -753,6 +753,80 @@ __device__ __forceinline__ float pq_distance(const uint8_t* __restrict__ code,
 // CosineNormalized, -dot table for InnerProduct (pq/distance/dynamic.rs:64-84).  Pivots are
 // read chunk-major (chunk m, centre c, len_m floats), so consecutive threads read
 // consecutive 16-byte pieces.
+// PQ with the Cosine metric (`DirectCosine`, pq/distance/cosine.rs:27-70 →
+// fixed_chunk_pq_table.rs:32-56, 233-243): per chunk m, one CosineStateless pass (the
+// Strategy2x4 order of `subgroup_cosine`) over (query chunk, pivot[code[m]] chunk) from zero,
+// folded lane by lane into a running accumulator; the cosine of the total, distance 1 - sim.
+// One 8-lane subgroup per candidate; lane s is SIMD lane s.
+__device__ __forceinline__ float subgroup_pq_cosine(const SearchParams& P, const float* q,
+                                                    const uint8_t* __restrict__ code, uint32_t s,
+                                                    unsigned gmask) {
+  float tx = 0.f, ty = 0.f, tp = 0.f;
+  for (uint32_t m = 0; m < P.pq_chunks; ++m) {
+    const uint32_t start = __ldg(P.offsets + m), stop = __ldg(P.offsets + m + 1);
+    const uint32_t len = stop - start, nvec = len >> 3;
+    const float* pv = P.pivots + (size_t)__ldg(code + m) * P.dim + start;
+    const float* qq = q + start;
+    float x0 = 0.f, y0 = 0.f, p0 = 0.f, x1 = 0.f, y1 = 0.f, p1 = 0.f;
+    uint32_t k = 0;
+    for (; k + 1u < nvec; k += 2u) {
+      const float b0 = __ldg(pv + 8u * k + s), b1 = __ldg(pv + 8u * k + 8u + s);
+      const float a0 = qq[8u * k + s], a1 = qq[8u * k + 8u + s];
+      x0 = __fmaf_rn(a0, a0, x0);
+      y0 = __fmaf_rn(b0, b0, y0);
+      p0 = __fmaf_rn(a0, b0, p0);
+      x1 = __fmaf_rn(a1, a1, x1);
+      y1 = __fmaf_rn(b1, b1, y1);
+      p1 = __fmaf_rn(a1, b1, p1);
+    }
+    if (k < nvec) {
+      const float b0 = __ldg(pv + 8u * k + s), a0 = qq[8u * k + s];
+      x0 = __fmaf_rn(a0, a0, x0);
+      y0 = __fmaf_rn(b0, b0, y0);
+      p0 = __fmaf_rn(a0, b0, p0);
+    }
+    float cx = x0 + x1, cy = y0 + y1, cp = p0 + p1;
+    if (s < (len & 7u)) {
+      const float b = __ldg(pv + 8u * nvec + s), a = qq[8u * nvec + s];
+      cx = __fmaf_rn(a, a, cx);
+      cy = __fmaf_rn(b, b, cy);
+      cp = __fmaf_rn(a, b, cp);
+    }
+    tx = tx + cx;
+    ty = ty + cy;
+    tp = tp + cp;
+  }
+#pragma unroll
+  for (int o = 4; o > 0; o >>= 1) {
+    tx += __shfl_xor_sync(gmask, tx, o, 8);
+    ty += __shfl_xor_sync(gmask, ty, o, 8);
+    tp += __shfl_xor_sync(gmask, tp, o, 8);
+  }
+  const float denom = __fmul_rn(__fsqrt_rn(tx), __fsqrt_rn(ty));
+  float sim;
+  if (tx < 1.17549435e-38f || ty < 1.17549435e-38f) sim = 0.0f;
+  else sim = fmaxf(-1.0f, fminf(1.0f, __fdiv_rn(tp, denom)));
+  return 1.0f - sim;
+}
+
+// PQ scoring of ids[0..count): table lookups, or DirectCosine by 8-lane subgroups.
+template <int METRIC>
+__device__ __forceinline__ void score_pq(const SearchParams& P, const float* q, const float* table,
+                                         const uint32_t* ids, float* d, uint32_t count,
+                                         uint32_t tid, uint32_t nt) {
+  if constexpr (METRIC == DK_METRIC_COSINE) {
+    const uint32_t s = tid & 7u;
+    const unsigned gmask = 0xFFu << (8u * ((tid & 31u) >> 3));
+    for (uint32_t i = tid >> 3; i < count; i += nt >> 3) {
+      const float r = subgroup_pq_cosine(P, q, P.codes + (size_t)ids[i] * P.cstride, s, gmask);
+      if (s == 0) d[i] = r;
+    }
+  } else {
+    for (uint32_t i = tid; i < count; i += nt)
+      d[i] = pq_distance(P.codes + (size_t)ids[i] * P.cstride, table, P.pq_chunks);
+  }
+}
+
 template <int METRIC>
 __device__ __forceinline__ void build_table(const SearchParams& P, const float* q, float* table,
                                             uint32_t tid, uint32_t nt) {
@@ -827,8 +901,7 @@ __device__ __forceinline__ void cta_score(const SearchParams& P, const State& S,
                                           float* d, uint32_t count) {
   const uint32_t tid = threadIdx.x;
   if (MODE == kModePQ) {
-    for (uint32_t i = tid; i < count; i += NT)
-      d[i] = pq_distance(P.codes + (size_t)ids[i] * P.cstride, S.table, P.pq_chunks);
+    score_pq<METRIC>(P, S.q, S.table, ids, d, count, tid, NT);
   } else {
     const unsigned gmask = 0xFFu << (8u * ((tid & 31u) >> 3));
     if constexpr (MODE == kModeFP32) {
@@ -965,7 +1038,7 @@ __device__ bool cta_search(const SearchParams& P, const State& S, const VSet& vs
     M->size = M->cursor = M->cur = M->inserted = M->overflow = M->nvalid = 0;
   }
   __syncthreads();
-  if (MODE == kModePQ) {
+  if (MODE == kModePQ && METRIC != DK_METRIC_COSINE) {
     build_table<METRIC>(P, S.q, S.table, tid, NT);
     __syncthreads();
   }
@@ -1282,8 +1355,7 @@ __device__ __forceinline__ void warp_score(const SearchParams& P, const State& S
                                            const uint32_t* ids, float* d, uint32_t count,
                                            uint32_t lane) {
   if (MODE == kModePQ) {
-    for (uint32_t i = lane; i < count; i += 32u)
-      d[i] = pq_distance(P.codes + (size_t)ids[i] * P.cstride, S.table, P.pq_chunks);
+    score_pq<METRIC>(P, S.q, S.table, ids, d, count, lane, 32u);
   } else {
     const unsigned gmask = 0xFFu << (8u * (lane >> 3));
     if constexpr (MODE == kModeFP32) {
@@ -1359,7 +1431,7 @@ __device__ __forceinline__ void warp_query(const SearchParams& P, const State& S
   for (uint32_t i = lane; i < dpad; i += 32u) S.q[i] = i < P.dim ? qsrc[i] : 0.0f;
   vset.reset(lane);
   __syncwarp();
-  if (MODE == kModePQ) {
+  if (MODE == kModePQ && METRIC != DK_METRIC_COSINE) {
     build_table<METRIC>(P, S.q, S.table, lane, 32u);
     __syncwarp();
   }
@@ -1614,13 +1686,11 @@ int32_t plan_warp(dk_index* ix, SearchParams& P, LaunchPlan& L, int mode, double
                   double est_mean, uint64_t max_warps, cudaStream_t stream);
 cudaError_t dispatch(int32_t metric, LaunchPlan& L, int mode, cudaStream_t stream);
 
-// All scoring modes of one metric (PQ traversal is not offered with the Cosine metric).
+// All scoring modes of one metric.
 template <int METRIC>
 cudaError_t launch_modes(LaunchPlan& L, int mode, cudaStream_t stream) {
   switch (mode) {
-    case kModePQ:
-      if (METRIC != DK_METRIC_COSINE) return launch_dims<METRIC, kModePQ>(L, stream);
-      return cudaErrorInvalidValue;
+    case kModePQ: return launch_dims<METRIC, kModePQ>(L, stream);
     case kModeBF16: return launch_dims<METRIC, kModeBF16>(L, stream);
     case kModeFP8: return launch_dims<METRIC, kModeFP8>(L, stream);
     default: return launch_dims<METRIC, kModeFP32>(L, stream);

@@ -303,6 +303,28 @@ inline float pq_lookup(const std::vector<float>& table, const uint8_t* code, uin
   return acc;
 }
 
+// PQ with the Cosine metric: `DirectCosine` (pq/distance/dynamic.rs:80, cosine.rs:27-70) →
+// `FixedChunkPQTable::cosine_distance` (fixed_chunk_pq_table.rs:233-243) →
+// `direct_distance_impl::<ResumableCosine>` (fixed_chunk_pq_table.rs:32-56): for every chunk m
+// one CosineStateless `simd_op` over (query[start..stop], pivot[code[m]][start..stop]) from a
+// fresh accumulator, folded into the running one lane by lane (`combine_with`: self + chunk,
+// simd.rs:3184-3190), then `sum` (the cosine similarity); distance = 1 - similarity.
+float pq_direct_cosine(const orc_index* ix, const float* q, const uint8_t* code) {
+  CosAcc total;
+  std::memset(&total, 0, sizeof(total));
+  for (uint32_t m = 0; m < ix->pq_chunks; ++m) {
+    const uint32_t start = ix->pq_offsets[m], stop = ix->pq_offsets[m + 1];
+    const float* pivot = ix->pq_pivots + (size_t)code[m] * ix->dim;
+    const CosAcc a = cosine_accumulate_v3(q + start, pivot + start, stop - start);
+    for (int l = 0; l < 8; ++l) {
+      total.x[l] = total.x[l] + a.x[l];
+      total.y[l] = total.y[l] + a.y[l];
+      total.xy[l] = total.xy[l] + a.xy[l];
+    }
+  }
+  return 1.0f - cosine_sum_v3(total);
+}
+
 struct Scorer {
   const orc_index* ix;
   const float* query;
@@ -310,8 +332,11 @@ struct Scorer {
   std::vector<float> table;
 
   float operator()(uint32_t id) const {
-    if (pq)
-      return pq_lookup(table, ix->pq_codes + (size_t)id * ix->pq_code_stride, ix->pq_chunks);
+    if (pq) {
+      const uint8_t* code = ix->pq_codes + (size_t)id * ix->pq_code_stride;
+      if (ix->metric == ORC_METRIC_COSINE) return pq_direct_cosine(ix, query, code);
+      return pq_lookup(table, code, ix->pq_chunks);
+    }
     return orc_distance(ix->metric, query, vec_row(ix, id), ix->dim);
   }
 };
@@ -352,7 +377,7 @@ extern "C" int32_t orc_search(const orc_index* ix, int32_t strategy, const float
   if (pq && ix->pq_chunks == 0) return ORC_ERR_NO_PQ;
 
   Scorer score{ix, query, pq, {}};
-  if (pq) pq_table(ix, query, score.table);
+  if (pq && ix->metric != ORC_METRIC_COSINE) pq_table(ix, query, score.table);
 
   const uint32_t n_start = ix->num_frozen;
   Queue best((size_t)l + n_start);

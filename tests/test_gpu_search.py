@@ -86,7 +86,8 @@ def test_full_precision_parity_benchmark_dims(dim, kernel):
     assert_same(gpu, orc.search(q, 10, 100, 1, O.STRATEGY_FULL_PRECISION, threads=4))
 
 
-@pytest.mark.parametrize("metric", [Metric.L2, Metric.INNER_PRODUCT, Metric.COSINE_NORMALIZED])
+@pytest.mark.parametrize("metric", [Metric.L2, Metric.INNER_PRODUCT, Metric.COSINE_NORMALIZED,
+                                    Metric.COSINE])
 @pytest.mark.parametrize("strategy", ["hybrid", "quantized"])
 def test_pq_parity(metric, strategy, kernel):
     norm = metric != Metric.L2
@@ -98,6 +99,20 @@ def test_pq_parity(metric, strategy, kernel):
     s, os_ = STRAT[strategy]
     for k, l, bw in [(10, 50, 1), (10, 100, 2), (5, 200, 1)]:
         assert_same(idx.search(Knn(k, l, bw), s, q), orc.search(q, k, l, bw, os_, threads=4))
+
+
+@pytest.mark.parametrize("dim,chunks", [(100, 7), (128, 8), (96, 5)])
+def test_pq_direct_cosine_parity(dim, chunks, kernel):
+    """PQ traversal with the Cosine metric (DirectCosine over the pivot chunks): chunk lengths
+    of 8 and more run the Strategy2x4 main loop, ragged ones the masked remainder."""
+    v, a, d, n = random_index(2500, dim, 24, seed=dim + chunks, max_degree=31)
+    off, piv, codes = simple_pq(v, chunks, seed=3)
+    q = queries_like(v[:n], 40, seed=4)
+    idx = DiskANNIndex(GpuProvider(v, a, d, n, Metric.COSINE, pq=PQData(off, piv, codes)))
+    orc = O.OracleIndex(v, a, d, n, O.METRIC_COSINE, off, piv, codes)
+    for strategy in ("quantized", "hybrid"):
+        s, os_ = STRAT[strategy]
+        assert_same(idx.search(Knn(10, 60, 1), s, q), orc.search(q, 10, 60, 1, os_, threads=4))
 
 
 def test_spill_pass_is_exact(monkeypatch, kernel):

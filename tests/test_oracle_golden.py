@@ -192,3 +192,58 @@ def test_oracle_accumulation_orders(n):
         assert got_l2.view(np.uint32) == _strategy_4x1(x, y, True).view(np.uint32)
         assert got_ip.view(np.uint32) == np.float32(-_strategy_4x1(x, y, False)).view(np.uint32)
         assert got_cos.view(np.uint32) == _cosine_2x4(x, y).view(np.uint32)
+
+
+def _direct_cosine(q, pivots, offsets, code):
+    """DirectCosine (fixed_chunk_pq_table.rs:32-56, 233-243): per chunk one CosineStateless
+    pass from zero, folded lane by lane into the running accumulator, then `sum`."""
+    total = np.zeros((3, 8), np.float32)
+    for m in range(len(offsets) - 1):
+        a0, a1 = int(offsets[m]), int(offsets[m + 1])
+        x, y = q[a0:a1], pivots[int(code[m])][a0:a1]
+        n = len(x)
+        acc = np.zeros((3, 2, 8), np.float32)
+        for k in range(n // 8):
+            for lane in range(8):
+                a, b = x[8 * k + lane], y[8 * k + lane]
+                acc[0][k % 2][lane] = _fma(a, a, acc[0][k % 2][lane])
+                acc[1][k % 2][lane] = _fma(b, b, acc[1][k % 2][lane])
+                acc[2][k % 2][lane] = _fma(a, b, acc[2][k % 2][lane])
+        t = [[_f32(acc[i][0][j] + acc[i][1][j]) for j in range(8)] for i in range(3)]
+        base = n - n % 8
+        for lane in range(n % 8):
+            a, b = x[base + lane], y[base + lane]
+            t[0][lane] = _fma(a, a, t[0][lane])
+            t[1][lane] = _fma(b, b, t[1][lane])
+            t[2][lane] = _fma(a, b, t[2][lane])
+        for i in range(3):
+            for j in range(8):
+                total[i][j] = _f32(total[i][j] + t[i][j])
+    nx, ny, xy = _sum_tree(total[0]), _sum_tree(total[1]), _sum_tree(total[2])
+    if nx < 1.17549435e-38 or ny < 1.17549435e-38:
+        sim = np.float32(0.0)
+    else:
+        den = _f32(_f32(np.sqrt(nx)) * _f32(np.sqrt(ny)))
+        sim = np.float32(max(-1.0, min(1.0, float(_f32(xy / den)))))
+    return _f32(np.float32(1.0) - sim)
+
+
+@pytest.mark.parametrize("dim,chunks", [(64, 16), (100, 7), (128, 8)])
+def test_oracle_pq_direct_cosine(dim, chunks):
+    """The oracle's Quantized search with the Cosine metric returns DirectCosine distances."""
+    rng = np.random.default_rng(dim)
+    n = 40
+    base = rng.standard_normal((n, dim)).astype(np.float32)
+    vectors = np.vstack([base, base[:1]])
+    adj = np.array([[j for j in range(n + 1) if j != i][:n] for i in range(n + 1)], np.uint32)
+    deg = np.full(n + 1, n, np.uint32)
+    offsets = np.linspace(0, dim, chunks + 1).round().astype(np.uint32)
+    pivots = rng.standard_normal((256, dim)).astype(np.float32)
+    codes = rng.integers(0, 256, size=(n + 1, chunks)).astype(np.uint8)
+    orc = O.OracleIndex(vectors, adj, deg, n, O.METRIC_COSINE, offsets, pivots, codes)
+    q = rng.standard_normal((3, dim)).astype(np.float32)
+    ids, dists, _ = orc.search(q, 10, 20, 1, O.STRATEGY_QUANTIZED)
+    for i in range(q.shape[0]):
+        for j in range(10):
+            want = _direct_cosine(q[i], pivots, offsets, codes[ids[i, j]])
+            assert dists[i, j].view(np.uint32) == want.view(np.uint32)
