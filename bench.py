@@ -40,6 +40,10 @@ WORKLOADS = {
     "fp100k": dict(n=100_000, dim=128, comps=64, sigma=10.0, nq=1000, R=32, l_build=50,
                    alpha=1.2, pq_chunks=0, pq_train=0, k=10, l_sweep=[50, 75, 100, 150, 200],
                    strategies=["fp32", "bf16", "fp8"], seed=0xD15CA77),
+    # A few thousand points: the CPU-only multi-rank tests and smoke runs.
+    "tiny": dict(n=3_000, dim=32, comps=8, sigma=5.0, nq=64, R=16, l_build=32, alpha=1.2,
+                 pq_chunks=8, pq_train=3_000, k=10, l_sweep=[20, 40, 80],
+                 strategies=["fp32", "bf16", "fp8", "hybrid"], seed=0xD15CA77 + 21),
     "pq100k": dict(n=100_000, dim=128, comps=256, sigma=8.0, nq=10_000, R=64, l_build=100,
                    alpha=1.2, pq_chunks=32, pq_train=100_000, k=10,
                    l_sweep=[50, 75, 100, 150, 200, 250, 300, 400],
@@ -483,12 +487,14 @@ def barrier(world):
 
 
 def max_over_ranks(x: float, world: int) -> float:
+    """Largest value over the ranks (timings are reported as the slowest rank's)."""
     if world <= 1:
         return x
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 

@@ -49,6 +49,11 @@
 namespace dk {
 
 constexpr uint32_t kEmpty = 0xFFFFFFFFu;
+
+// Minimum resident 128-thread blocks per SM the warp kernel is compiled for (caps registers).
+#ifndef DK_WARP_MIN_BLOCKS
+#define DK_WARP_MIN_BLOCKS 1
+#endif
 constexpr uint32_t kVisited = 0x80000000u;
 constexpr uint32_t kIdMask = 0x7FFFFFFFu;
 constexpr uint32_t kFull = 0xFFFFFFFFu;
@@ -1563,7 +1568,7 @@ __device__ __forceinline__ void warp_query(const SearchParams& P, const State& S
 // Persistent grid: every warp owns a shared-memory slice and a global overflow table and
 // takes queries from a work counter until the batch is done.
 template <int METRIC, int MODE, int DIM, int U>
-__global__ void __launch_bounds__(128) k_search_warp(const SearchParams P) {
+__global__ void __launch_bounds__(128, DK_WARP_MIN_BLOCKS) k_search_warp(const SearchParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
   const uint32_t slot = blockIdx.x * (blockDim.x >> 5) + warp;
