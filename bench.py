@@ -233,38 +233,37 @@ def stats_array(st):
     return out
 
 
-def serve_latency(provider, strategy, queries, k, l, rate, seconds, seed=1):
-    """Poisson arrivals at `rate` requests/s through the serving API (dk_server_*); latency is
-    completion seen by the host minus scheduled arrival.  Returns p50/p99 (ms) and the rate
-    achieved."""
+def serve_latency(provider, strategy, queries, gt, k, l, rate, seconds, mixed=False, seed=1):
+    """Poisson arrivals at `rate` requests/s replayed natively through the serving API
+    (dk_server_replay from one host thread); latency = completion seen by the host - scheduled
+    arrival.  `mixed`: each request draws k from {10, 50, 100} and L from {64, 128, 256, 512}
+    (L >= k), as in the served-stream config; else every request uses (k, l)."""
     from diskann_b200 import SearchServer
+    from diskann_b200.groundtruth import recall_at_k
 
-    srv = SearchServer(provider, strategy, max_k=k, max_l=l, queue_depth=8192)
-    nq = queries.shape[0]
-    srv.wait(srv.submit(queries[0], k, l), k)
+    rng = np.random.default_rng(seed)
     n = max(1, int(rate * seconds))
-    arrivals = np.cumsum(np.random.default_rng(seed).exponential(1.0 / rate, size=n))
-    lat = np.zeros(n)
-    outstanding = {}
-    i = done = 0
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n))
+    if mixed:
+        ks = rng.choice([10, 50, 100], size=n)
+        ls = np.maximum(rng.choice([64, 128, 256, 512], size=n), ks)
+    else:
+        ks = np.full(n, k)
+        ls = np.full(n, l)
+    srv = SearchServer(provider, strategy, max_k=int(ks.max()), max_l=int(ls.max()),
+                       queue_depth=16384)
+    srv.replay(queries[:64], ks[:64], ls[:64], np.zeros(64))  # warm-up
     t0 = time.perf_counter()
-    while done < n:
-        now = time.perf_counter() - t0
-        while i < n and arrivals[i] <= now:
-            outstanding[srv.submit(queries[i % nq], k, l)] = i
-            i += 1
-        for t in list(outstanding):
-            if srv.poll(t, k) is not None:
-                j = outstanding.pop(t)
-                lat[j] = time.perf_counter() - t0 - arrivals[j]
-                done += 1
-        if time.perf_counter() - t0 > seconds * 4 + 10:
-            break
+    lat, ids, _ = srv.replay(queries, ks, ls, arrivals, want_results=True)
     elapsed = time.perf_counter() - t0
     info = srv.info()
     srv.close()
-    pct = percentiles(lat[:done] * 1e3)
-    return {"offered_qps": rate, "achieved_qps": round(done / elapsed, 1), "requests": done,
+    rows = np.arange(n) % queries.shape[0]
+    rec = recall_at_k(ids[:, :10], gt[rows], 10)
+    pct = percentiles(lat * 1e3)
+    return {"offered_qps": rate, "achieved_qps": round(n / elapsed, 1), "requests": n,
+            "stream": "mixed k in {10,50,100}, L in {64,128,256,512}" if mixed else f"k={k}, L={l}",
+            "recall_at_10": round(rec, 4),
             "p50_ms": round(pct["median"], 4), "p90_ms": round(pct["p90"], 4),
             "p99_ms": round(pct["p99"], 4), "mean_ms": round(pct["mean"], 4),
             "launches": int(info["launches"]), "streams": int(info["streams"])}
@@ -382,11 +381,14 @@ def run_ours(args, data, rank, world):
             e2e_t.append(t1 - t0)
     e2e_s = max_over_ranks(float(np.mean(e2e_t)) * 1e3, world) / 1e3
 
-    # Serving: Poisson arrivals through dk_server_* at two offered rates (rank 0 of N=1 only).
+    # Serving: Poisson arrivals replayed through dk_server_* at several offered rates, and a
+    # mixed-k/L stream (N=1 only).
     serving = None
     if world == 1 and not args.no_serving:
-        serving = [serve_latency(provider, strategy, queries, k, chosen, rate, args.serve_seconds)
-                   for rate in (2000.0, 20000.0)]
+        serving = [serve_latency(provider, strategy, queries, gt, k, chosen, rate, args.serve_seconds)
+                   for rate in (10_000.0, 100_000.0, 500_000.0, 1_000_000.0)]
+        serving.append(serve_latency(provider, strategy, queries, gt, k, chosen, 100_000.0,
+                                     args.serve_seconds, mixed=True))
         log(f"[ours] serving {serving}")
 
     mean_deg = float(data["deg"][: data["n"]].mean())
@@ -560,7 +562,7 @@ def main():
     ap.add_argument("--cache", default=os.environ.get("DK_BENCH_CACHE", "/tmp/diskann_b200_bench"))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
-    ap.add_argument("--serve-seconds", type=float, default=2.0)
+    ap.add_argument("--serve-seconds", type=float, default=1.0)
     ap.add_argument("--profile", default=None, metavar="STRATEGY:L",
                     help="profiling case for ncu: upload the workload's index and run two "
                          "batched searches (warm-up, profiled), no timing, no JSON line")

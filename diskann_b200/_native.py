@@ -28,6 +28,7 @@ EXPORTED_SYMBOLS = (
     "dk_server_create",
     "dk_server_submit",
     "dk_server_poll",
+    "dk_server_replay",
     "dk_server_get_info",
     "dk_server_destroy",
     "dk_distance",
@@ -140,6 +141,8 @@ def load():
         L.dk_server_submit.argtypes = [vp, vp, u32, u32, ctypes.POINTER(u64)]
         L.dk_server_poll.restype = i32
         L.dk_server_poll.argtypes = [vp, u64, vp, vp, vp]
+        L.dk_server_replay.restype = i32
+        L.dk_server_replay.argtypes = [vp, vp, u64, u32, vp, vp, vp, u32, vp, vp, vp]
         L.dk_server_get_info.restype = i32
         L.dk_server_get_info.argtypes = [vp, ctypes.POINTER(ServerInfo)]
         L.dk_server_destroy.restype = i32

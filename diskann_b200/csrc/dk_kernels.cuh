@@ -50,10 +50,13 @@ namespace dk {
 
 constexpr uint32_t kEmpty = 0xFFFFFFFFu;
 
-// Minimum resident 128-thread blocks per SM the warp kernel is compiled for (caps registers).
-#ifndef DK_WARP_MIN_BLOCKS
-#define DK_WARP_MIN_BLOCKS 1
-#endif
+// Minimum resident 128-thread blocks per SM the warp kernel is compiled for, which caps its
+// registers: the low-precision kernels run faster capped at 80 registers (more resident warps),
+// the FP32 kernel uncapped (its four-row scoring rounds need the registers).  Measured on pq1m.
+template <int MODE>
+constexpr int warp_min_blocks() {
+  return (MODE == kModeBF16 || MODE == kModeFP8) ? 6 : 1;
+}
 constexpr uint32_t kVisited = 0x80000000u;
 constexpr uint32_t kIdMask = 0x7FFFFFFFu;
 constexpr uint32_t kFull = 0xFFFFFFFFu;
@@ -1568,7 +1571,7 @@ __device__ __forceinline__ void warp_query(const SearchParams& P, const State& S
 // Persistent grid: every warp owns a shared-memory slice and a global overflow table and
 // takes queries from a work counter until the batch is done.
 template <int METRIC, int MODE, int DIM, int U>
-__global__ void __launch_bounds__(128, DK_WARP_MIN_BLOCKS) k_search_warp(const SearchParams P) {
+__global__ void __launch_bounds__(128, warp_min_blocks<MODE>()) k_search_warp(const SearchParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
   const uint32_t slot = blockIdx.x * (blockDim.x >> 5) + warp;
@@ -1614,7 +1617,8 @@ struct LaunchPlan {
   uint32_t warps_per_cta;
   uint32_t grid;       // warp kernel: persistent grid size
   uint32_t spill_ctas;
-  uint32_t score_u;    // warp kernel, D <= 128: rows per subgroup per round (2 or 4)
+  uint32_t score_u;    // warp kernel, D <= 128: FP32 rows per subgroup per round (2 or 4; the
+                       // FP32 rerank of the low-precision kernels uses it too)
   bool query_only;     // warp kernel: only report `blocks_per_sm` for `warps_per_cta`
   bool skip_spill;     // serving launches: spilled requests are re-run by the host
   int blocks_per_sm;

@@ -130,7 +130,7 @@ extern "C" int32_t dk_search_device_noalloc(dk_index* ix, int32_t strategy, cons
   if (256 + per_bitmap > cap_bytes) return too_big_scratch(256 + per_bitmap);
   uint32_t spill_ctas = std::min<uint32_t>(nq, (uint32_t)std::max(1, sms));
   dk::LaunchPlan L{};
-  L.score_u = env_u32("DK_SCORE_U", 2);
+  L.score_u = env_u32("DK_SCORE_U", mode == kModeFP32 ? 4u : 2u);
   uint64_t off_bitmap = 256;
   if (warp) {
     L.kind = dk::KernelKind::kWarp;

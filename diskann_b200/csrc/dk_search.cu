@@ -209,7 +209,7 @@ int32_t dk_launch_search(dk_index* ix, int32_t strategy, const float* queries,
   if (kenv && !strcmp(kenv, "cta")) warp = false;
 
   dk::LaunchPlan L{};
-  L.score_u = env_u32("DK_SCORE_U", 2);
+  L.score_u = env_u32("DK_SCORE_U", mode == kModeFP32 ? 4u : 2u);
   uint64_t gtable_bytes = 0;
   cudaError_t e = cudaSuccess;
   if (warp) {

@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstdint>
 #include <cstring>
 #include <deque>
@@ -224,7 +225,7 @@ extern "C" int32_t dk_server_create(dk_index* ix, const dk_server_config* cfg, d
   double est = 0, est_mean = 0;
   dk::visited_estimates(ix, P, est, est_mean);
   s->plan.kind = dk::KernelKind::kWarp;
-  s->plan.score_u = 2;
+  s->plan.score_u = s->mode == kModeFP32 ? 4u : 2u;
   s->plan.skip_spill = true;
   const uint64_t max_warps = cfg->max_slots ? cfg->max_slots : (1ull << 32);
   v = dk::plan_warp(ix, P, s->plan, s->mode, est, est_mean, max_warps, nullptr);
@@ -351,6 +352,96 @@ extern "C" int32_t dk_server_poll(dk_server* s, uint64_t ticket, uint32_t* ids, 
   if (stats) *stats = st;
   s->state[r] = kFree;
   while (s->head < s->next_ticket && s->state[s->head % depth] == kFree) ++s->head;
+  return DK_OK;
+}
+
+extern "C" int32_t dk_server_replay(dk_server* s, const float* queries, uint64_t query_stride,
+                                    uint32_t nq, const uint32_t* ks, const uint32_t* ls,
+                                    const uint64_t* arrival_ns, uint32_t n, uint64_t* latency_ns,
+                                    uint32_t* ids, float* dists) {
+  if (!s || !queries || !ks || !ls || !arrival_ns || !latency_ns || (n && nq == 0))
+    return fail(DK_ERR_INVALID_ARGUMENT, "server, queries, k, L, arrivals and latencies are required");
+  if (query_stride < s->ix->dim) return fail(DK_ERR_DIMENSION_MISMATCH, "query stride below dim");
+  for (uint32_t i = 0; i < n; ++i) {
+    const int32_t v = dk_knn_validate(ks[i], ls[i], s->cfg.beam_width);
+    if (v != DK_OK) return v;
+    if (ks[i] > s->cfg.max_k || ls[i] > s->cfg.max_l)
+      return fail(DK_ERR_INVALID_ARGUMENT, "k or L above the server's max_k / max_l");
+    if (i && arrival_ns[i] < arrival_ns[i - 1])
+      return fail(DK_ERR_INVALID_ARGUMENT, "arrival times must not decrease");
+  }
+  const uint32_t max_k = s->cfg.max_k, depth = s->cfg.queue_depth, dim = s->ix->dim;
+  std::vector<std::pair<uint64_t, uint32_t>> out;  // (ticket, request) in flight
+  out.reserve(std::min<uint32_t>(n, depth));
+  std::vector<uint64_t> keep;
+  const auto t0 = std::chrono::steady_clock::now();
+  auto now_ns = [&]() {
+    return (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
+               std::chrono::steady_clock::now() - t0).count();
+  };
+  uint32_t next = 0, done = 0;
+  DeviceGuard guard(s->ix->device);
+  while (done < n) {
+    std::lock_guard<std::mutex> lock(s->mu);
+    // Submit every request whose arrival time has come, while admission allows.
+    const uint64_t now = now_ns();
+    while (next < n && arrival_ns[next] <= now && s->next_ticket - s->head < depth) {
+      const uint64_t t = s->next_ticket++;
+      const uint32_t r = (uint32_t)(t % depth);
+      s->req_k[r] = ks[next];
+      s->req_l[r] = ls[next];
+      memcpy(&s->queries[(size_t)r * dim], queries + (size_t)(next % nq) * query_stride, 4ull * dim);
+      s->state[r] = kPending;
+      s->pending.push_back(t);
+      out.emplace_back(t, next);
+      ++next;
+    }
+    const int32_t rc = progress(s);
+    if (rc != DK_OK) return rc;
+    // Collect what is done, in any order.
+    size_t w = 0;
+    for (size_t j = 0; j < out.size(); ++j) {
+      const uint64_t t = out[j].first;
+      const uint32_t i = out[j].second, r = (uint32_t)(t % depth);
+      if (s->state[r] != kDone || (s->res_stats[r].flags & kFlagSpilled)) {
+        if (s->state[r] == kDone) {
+          // Spilled: collect through the exact re-run of dk_server_poll (lock released there).
+          keep.push_back(t);
+        }
+        out[w++] = out[j];
+        continue;
+      }
+      const uint64_t fin = now_ns();
+      latency_ns[i] = fin > arrival_ns[i] ? fin - arrival_ns[i] : 0;
+      if (ids) memcpy(ids + (size_t)i * max_k, &s->res_ids[(size_t)r * max_k], 4ull * ks[i]);
+      if (dists) memcpy(dists + (size_t)i * max_k, &s->res_dists[(size_t)r * max_k], 4ull * ks[i]);
+      s->state[r] = kFree;
+      ++done;
+    }
+    out.resize(w);
+    while (s->head < s->next_ticket && s->state[s->head % depth] == kFree) ++s->head;
+    if (!keep.empty()) {
+      // Rare: a request whose visited tables overflowed is re-run exactly by the batch path.
+      std::vector<uint32_t> tid(max_k);
+      std::vector<float> td(max_k);
+      for (uint64_t t : keep) {
+        size_t j = 0;
+        while (out[j].first != t) ++j;
+        const uint32_t i = out[j].second;
+        s->mu.unlock();
+        const int32_t prc = dk_server_poll(s, t, tid.data(), td.data(), nullptr);
+        s->mu.lock();
+        if (prc != DK_OK) return prc;
+        const uint64_t fin = now_ns();
+        latency_ns[i] = fin > arrival_ns[i] ? fin - arrival_ns[i] : 0;
+        if (ids) memcpy(ids + (size_t)i * max_k, tid.data(), 4ull * ks[i]);
+        if (dists) memcpy(dists + (size_t)i * max_k, td.data(), 4ull * ks[i]);
+        out.erase(out.begin() + (long)j);
+        ++done;
+      }
+      keep.clear();
+    }
+  }
   return DK_OK;
 }
 

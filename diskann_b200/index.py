@@ -329,6 +329,25 @@ class SearchServer:
                 raise TimeoutError(f"request {ticket} not done after {timeout_s} s")
             time.sleep(0)
 
+    def replay(self, queries, ks, ls, arrival_s, want_results: bool = False):
+        """Replay a request stream natively (``dk_server_replay``): request i uses query row
+        i % len(queries), ks[i], ls[i] and arrives arrival_s[i] seconds after the start.
+        Returns latencies in seconds (and ``(ids, dists)`` with ``want_results``)."""
+        q = np.ascontiguousarray(np.atleast_2d(queries), dtype=np.float32)
+        ks = np.ascontiguousarray(ks, dtype=np.uint32)
+        ls = np.ascontiguousarray(ls, dtype=np.uint32)
+        arr = np.ascontiguousarray(np.round(np.asarray(arrival_s) * 1e9), dtype=np.uint64)
+        n = len(arr)
+        lat = np.zeros(n, dtype=np.uint64)
+        ids = np.empty((n, self.max_k), np.uint32) if want_results else None
+        dists = np.empty((n, self.max_k), np.float32) if want_results else None
+        _check(_native.load().dk_server_replay(
+            self.handle, q.ctypes.data, q.shape[1], q.shape[0], ks.ctypes.data, ls.ctypes.data,
+            arr.ctypes.data, n, lat.ctypes.data, None if ids is None else ids.ctypes.data,
+            None if dists is None else dists.ctypes.data))
+        lat_s = lat.astype(np.float64) / 1e9
+        return (lat_s, ids, dists) if want_results else lat_s
+
     def info(self) -> dict:
         inf = _native.ServerInfo()
         _check(_native.load().dk_server_get_info(self.handle, ctypes.byref(inf)))

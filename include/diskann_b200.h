@@ -226,6 +226,17 @@ int32_t dk_server_submit(dk_server* server, const float* query, uint32_t k, uint
                          uint64_t* ticket);
 int32_t dk_server_poll(dk_server* server, uint64_t ticket, uint32_t* ids, float* dists,
                        dk_search_stats* stats);
+/* Load-test driver (no counterpart in the reference; the role of its benchmark runner): replay
+ * a request stream through the server from the calling host thread.  Request i uses query row
+ * i % nq, k[i] and L[i], and is submitted arrival_ns[i] nanoseconds after the call starts (not
+ * decreasing; a request that finds queue_depth requests outstanding waits for admission);
+ * latency_ns[i] = when the calling thread sees its results - arrival_ns[i].  ids / dists (may
+ * be NULL) receive n x max_k entries.  The thread spins between events; returns when every
+ * request is done. */
+int32_t dk_server_replay(dk_server* server, const float* queries, uint64_t query_stride,
+                         uint32_t nq, const uint32_t* k, const uint32_t* l,
+                         const uint64_t* arrival_ns, uint32_t n, uint64_t* latency_ns,
+                         uint32_t* ids, float* dists);
 int32_t dk_server_get_info(const dk_server* server, dk_server_info* info);
 int32_t dk_server_destroy(dk_server* server);
 

@@ -134,3 +134,23 @@ def test_admission_and_errors():
     info = srv.info()
     assert info["slots"] > 0 and info["queue_depth"] == 4 and info["streams"] == 2
     srv.close()
+
+
+def test_native_replay_matches_the_oracle_under_load():
+    v, a, d, n = random_index(4000, 64, 24, seed=16)
+    q = queries_like(v[:n], 200, seed=10)
+    orc = O.OracleIndex(v, a, d, n, O.METRIC_L2)
+    srv = SearchServer(GpuProvider(v, a, d, n, Metric.L2), FullPrecision(), max_k=20, max_l=120,
+                       queue_depth=64)
+    rng = np.random.default_rng(17)
+    ks = rng.integers(1, 21, size=600)
+    ls = np.array([int(rng.integers(k, 121)) for k in ks])
+    arrivals = np.cumsum(rng.exponential(1.0 / 50000.0, size=600))  # 50k requests/s
+    lat, ids, dists = srv.replay(q, ks, ls, arrivals, want_results=True)
+    assert (lat > 0).all() and (lat < 10.0).all()
+    for i in range(0, 600, 7):
+        oi, od, _ = orc.search(q[i % 200 : i % 200 + 1], int(ks[i]), int(ls[i]), 1,
+                               O.STRATEGY_FULL_PRECISION)
+        np.testing.assert_array_equal(ids[i, : ks[i]], oi[0])
+        np.testing.assert_array_equal(dists[i, : ks[i]].view(np.uint32), od[0].view(np.uint32))
+    srv.close()
