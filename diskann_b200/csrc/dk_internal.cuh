@@ -80,6 +80,7 @@ struct SearchParams {
   // Warp kernel: persistent work counter and each warp's global overflow hash (second level
   // of the visited set, used once the shared hash holds `hash_limit` ids).
   uint32_t* work_counter;
+  uint32_t* spill_count;  // queries the first pass abandoned (the spill pass exits at 0); may be null
   uint32_t* gtable;
   uint32_t gtable_log2;
   uint32_t gtable_limit;

@@ -1121,7 +1121,10 @@ __global__ void __launch_bounds__(NT) k_search_cta(const SearchParams P) {
   if (qid >= P.nq) return;
   uint32_t cmps = 0, hops = 0;
   if (!cta_search<NT, METRIC, MODE, DIM>(P, S, vset, qid, cmps, hops)) {
-    if (threadIdx.x == 0) P.stats[qid] = dk_search_stats{0u, 0u, 0u, kFlagSpilled};
+    if (threadIdx.x == 0) {
+      P.stats[qid] = dk_search_stats{0u, 0u, 0u, kFlagSpilled};
+      if (P.spill_count) atomicAdd(P.spill_count, 1u);
+    }
     return;
   }
   cta_post_process<NT, METRIC, DIM>(P, S, qid);
@@ -1138,6 +1141,7 @@ __global__ void __launch_bounds__(NT) k_search_spill(const SearchParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
   const State S = carve(smem, P);
   BitmapSet vset{P.bitmap + (size_t)blockIdx.x * P.bitmap_words, P.bitmap_words};
+  if (P.spill_count && *(volatile const uint32_t*)P.spill_count == 0u) return;  // nothing spilled
   for (uint32_t qid = blockIdx.x; qid < P.nq; qid += gridDim.x) {
     if (!(P.stats[qid].flags & kFlagSpilled)) continue;
     __syncthreads();
@@ -1444,7 +1448,10 @@ __device__ __forceinline__ void warp_query(const SearchParams& P, const State& S
     __syncwarp();
   }
   if (P.f + P.beam * P.max_degree > P.gtable_limit) {
-    if (lane == 0) *io.stats = dk_search_stats{0u, 0u, 0u, kFlagSpilled};
+    if (lane == 0) {
+      *io.stats = dk_search_stats{0u, 0u, 0u, kFlagSpilled};
+      if (P.spill_count) atomicAdd(P.spill_count, 1u);
+    }
     return;
   }
   uint32_t size = 0, cursor = 0, cur = 0;
@@ -1490,7 +1497,10 @@ __device__ __forceinline__ void warp_query(const SearchParams& P, const State& S
     __syncwarp();
     // The global level must keep room for a whole hop going there; otherwise spill.
     if (vset.gcount + nb * P.max_degree > P.gtable_limit) {
-      if (lane == 0) *io.stats = dk_search_stats{0u, 0u, 0u, kFlagSpilled};
+      if (lane == 0) {
+      *io.stats = dk_search_stats{0u, 0u, 0u, kFlagSpilled};
+      if (P.spill_count) atomicAdd(P.spill_count, 1u);
+    }
       return;
     }
     // Expand: adjacency rows in beam order, ids through the visited set in order.

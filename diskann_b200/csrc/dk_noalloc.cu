@@ -166,8 +166,10 @@ extern "C" int32_t dk_search_device_noalloc(dk_index* ix, int32_t strategy, cons
 
   cudaError_t e = cudaMemsetAsync(scratch, 0, 256, stream);  // the work counter starts at 0
   P.work_counter = reinterpret_cast<uint32_t*>(scratch);
+  P.spill_count = reinterpret_cast<uint32_t*>(scratch) + 1;  // zeroed with the counter
   P.gtable = reinterpret_cast<uint32_t*>(scratch + 256);
   P2.bitmap = reinterpret_cast<uint32_t*>(scratch + off_bitmap);
+  P2.spill_count = P.spill_count;
   P2.bitmap_words = words;
   L.p1 = P;
   L.p2 = P2;
