@@ -82,9 +82,14 @@ def prepare(name: str, rank: int, cache_root: str):
                                                   seed=w["seed"], n_queries=w["nq"])
         log(f"[prepare] data {time.time() - t0:.1f}s")
         t0 = time.time()
+        import torch
+
+        # Larger batches search on the GPU when there is one: the same graph as the host build.
+        dev = 0 if torch.cuda.is_available() else None
         vectors, adj, deg, n = graph.build_vamana(base, pruned_degree=w["R"], l_build=w["l_build"],
-                                                  alpha=w["alpha"])
-        log(f"[prepare] vamana build {time.time() - t0:.1f}s, mean degree {deg[:n].mean():.1f}")
+                                                  alpha=w["alpha"], device=dev)
+        log(f"[prepare] vamana build ({'GPU searches' if dev is not None else 'host'}) "
+            f"{time.time() - t0:.1f}s, mean degree {deg[:n].mean():.1f}")
         np.save(os.path.join(cdir, "vectors.npy"), vectors)
         np.save(os.path.join(cdir, "queries.npy"), queries)
         np.save(os.path.join(cdir, "adj.npy"), adj)

@@ -34,6 +34,7 @@ EXPORTED_SYMBOLS = (
     "dk_distance",
     "dk_compute_medoid",
     "dk_build_vamana",
+    "dk_build_vamana_device",
     "dk_pq_train",
     "dk_pq_encode",
 )

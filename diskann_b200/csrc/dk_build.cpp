@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "diskann_b200.h"
+#include "dk_build_gpu.h"
 #include "dk_internal.cuh"
 
 namespace {
@@ -310,10 +311,15 @@ extern "C" int32_t dk_compute_medoid(const float* vectors, uint64_t stride, uint
   return DK_OK;
 }
 
-extern "C" int32_t dk_build_vamana(const float* vectors, uint64_t stride, uint32_t num_points,
-                                   uint32_t num_frozen, uint32_t dim, int32_t metric,
-                                   const dk_build_params* params, uint32_t* adjacency,
-                                   uint64_t adjacency_stride, uint32_t* degrees) {
+namespace {
+
+// Batches at least this large search on the GPU when a device builder is given; smaller ones
+// (the first few, which grow 1, 2, 4, ...) search on the host threads.
+constexpr uint32_t kGpuMinBatch = 256;
+
+int32_t build_impl(const float* vectors, uint64_t stride, uint32_t num_points, uint32_t num_frozen,
+                   uint32_t dim, int32_t metric, const dk_build_params* params, uint32_t* adjacency,
+                   uint64_t adjacency_stride, uint32_t* degrees, int32_t device) {
   if (!vectors || !params || !adjacency || !degrees || dim == 0 || stride < dim ||
       num_frozen == 0) {
     dk_set_error(DK_ERR_INVALID_ARGUMENT, "invalid build arguments");
@@ -344,25 +350,57 @@ extern "C" int32_t dk_build_vamana(const float* vectors, uint64_t stride, uint32
   std::vector<BuildScratch> scratch(threads);
   for (auto& s : scratch) s.stamp.assign(total, 0u);
 
+  dk_build_gpu* gpu = nullptr;
+  if (device >= 0) {
+    const int32_t rc = dk_build_gpu_create(vectors, stride, num_points, num_frozen, dim, metric,
+                                           B.p.max_degree, B.p.l_build, B.p.max_batch, device, &gpu);
+    if (rc != DK_OK) return rc;
+  }
+  struct GpuGuard {
+    dk_build_gpu* g;
+    ~GpuGuard() { dk_build_gpu_destroy(g); }
+  } gpu_guard{gpu};
+
   std::vector<std::vector<uint32_t>> out;
+  std::vector<uint32_t> changed;
   uint32_t start = 0, bsize = 1;
   while (start < num_points) {
     const uint32_t end = std::min<uint32_t>(num_points, start + bsize);
     const uint32_t cnt = end - start;
     out.assign(cnt, {});
-    // Search + prune each point of the batch against the graph before the batch.
+    // The visited search record of every point of the batch against the graph before the
+    // batch: from the GPU for large batches (same search, bit-exact), else on the host.
+    const uint32_t* rec_ids = nullptr;
+    const float* rec_d = nullptr;
+    const uint32_t* hops = nullptr;
+    uint32_t rec_cap = 0;
+    if (gpu && cnt >= kGpuMinBatch) {
+      const int32_t rc = dk_build_gpu_search(gpu, start, cnt, &rec_ids, &rec_d, &hops, &rec_cap);
+      if (rc != DK_OK) return rc;
+    }
     parallel_for(threads, cnt, [&](uint64_t i, uint32_t w) {
       const uint32_t id = start + (uint32_t)i;
       BuildScratch& S = scratch[w];
-      B.search(id, S);
-      std::vector<Candidate> pool = S.visited_record;
+      std::vector<Candidate> pool;
+      if (rec_ids && hops[i] <= rec_cap) {
+        pool.reserve(hops[i]);
+        for (uint32_t h = 0; h < hops[i]; ++h)
+          pool.push_back({rec_ids[(size_t)i * rec_cap + h], rec_d[(size_t)i * rec_cap + h]});
+      } else {
+        B.search(id, S);
+        pool = S.visited_record;
+      }
       pool.erase(std::remove_if(pool.begin(), pool.end(),
                                 [&](const Candidate& c) { return c.id == id; }),
                  pool.end());
       Builder::sort_pool(pool, B.p.max_occlusion);
       B.occlude(id, pool, out[i]);
     });
-    for (uint32_t i = 0; i < cnt; ++i) B.adj[start + i] = out[i];
+    changed.clear();
+    for (uint32_t i = 0; i < cnt; ++i) {
+      B.adj[start + i] = out[i];
+      changed.push_back(start + i);
+    }
     // Back edges (add_edge_and_prune), grouped by target, sources in point order.
     std::vector<std::pair<uint32_t, uint32_t>> edges;  // (target, source)
     for (uint32_t i = 0; i < cnt; ++i) {
@@ -378,6 +416,7 @@ extern "C" int32_t dk_build_vamana(const float* vectors, uint64_t stride, uint32
       groups.emplace_back(a, b);
       a = b;
     }
+    std::vector<uint8_t> touched(groups.size(), 0);
     parallel_for(threads, groups.size(), [&](uint64_t g, uint32_t) {
       const uint32_t target = edges[groups[g].first].first;
       std::vector<uint32_t> lst = B.adj[target];
@@ -390,6 +429,7 @@ extern "C" int32_t dk_build_vamana(const float* vectors, uint64_t stride, uint32
         }
       }
       if (!added) return;
+      touched[g] = 1;
       if (lst.size() <= p.max_degree) {
         B.adj[target] = lst;
         return;
@@ -403,6 +443,15 @@ extern "C" int32_t dk_build_vamana(const float* vectors, uint64_t stride, uint32
       B.occlude(target, pool, pruned);
       B.adj[target] = pruned;
     });
+    if (gpu) {
+      for (size_t g = 0; g < groups.size(); ++g)
+        if (touched[g]) {
+          const uint32_t target = edges[groups[g].first].first;
+          if (target < start || target >= end) changed.push_back(target);
+        }
+      const int32_t rc = dk_build_gpu_set_rows(gpu, changed.data(), (uint32_t)changed.size(), B.adj);
+      if (rc != DK_OK) return rc;
+    }
     start = end;
     bsize = std::min<uint32_t>(bsize * 2, B.p.max_batch);
   }
@@ -414,6 +463,29 @@ extern "C" int32_t dk_build_vamana(const float* vectors, uint64_t stride, uint32
     std::copy(lst.begin(), lst.end(), dst);
   }
   return DK_OK;
+}
+
+}  // namespace
+
+extern "C" int32_t dk_build_vamana(const float* vectors, uint64_t stride, uint32_t num_points,
+                                   uint32_t num_frozen, uint32_t dim, int32_t metric,
+                                   const dk_build_params* params, uint32_t* adjacency,
+                                   uint64_t adjacency_stride, uint32_t* degrees) {
+  return build_impl(vectors, stride, num_points, num_frozen, dim, metric, params, adjacency,
+                    adjacency_stride, degrees, -1);
+}
+
+extern "C" int32_t dk_build_vamana_device(const float* vectors, uint64_t stride,
+                                          uint32_t num_points, uint32_t num_frozen, uint32_t dim,
+                                          int32_t metric, const dk_build_params* params,
+                                          uint32_t* adjacency, uint64_t adjacency_stride,
+                                          uint32_t* degrees, int32_t device) {
+  if (device < 0) {
+    dk_set_error(DK_ERR_INVALID_ARGUMENT, "device must be a CUDA device ordinal");
+    return DK_ERR_INVALID_ARGUMENT;
+  }
+  return build_impl(vectors, stride, num_points, num_frozen, dim, metric, params, adjacency,
+                    adjacency_stride, degrees, device);
 }
 
 // Chunk offsets: the first dim % chunks chunks are one longer (diskann-quantization

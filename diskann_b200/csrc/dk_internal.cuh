@@ -92,6 +92,11 @@ struct SearchParams {
   uint32_t warp_smem;
   uint32_t list_cap;  // capacity of the candidate / rerank lists
   uint32_t* hint;     // device words of the visited-size hint (may be null)
+  // Graph construction: the expanded nodes of each query in order, with their distances
+  // (the reference's visited search record), up to rec_cap per query; null when unused.
+  uint32_t* rec_ids;
+  float* rec_d;
+  uint32_t rec_cap;
   // Serving launches: per-request (k, L) pairs; outputs keep a stride of `k` (= max_k).
   // Null for batch launches, where every query uses `k` and `l`.
   const uint32_t* req_kl;
@@ -131,9 +136,18 @@ int32_t dk_check_search_args(const dk_index* ix, int32_t strategy, uint32_t k, u
 // Derive the low-precision copies requested by `flags` from the index's FP32 rows.
 cudaError_t dk_build_low_precision(dk_index* ix, uint32_t flags);
 
+// Optional output of dk_launch_search: each query's expanded nodes in order with their queue
+// distances (rec_cap per query; a query that expanded more than rec_cap nodes records the
+// first rec_cap, and its stats.hops tells).
+struct SearchRecord {
+  uint32_t* ids;
+  float* dists;
+  uint32_t cap;
+};
+
 // Launch the search (first pass + spill pass) on `stream`.  Parameters are validated by
 // the caller.
 int32_t dk_launch_search(dk_index* ix, int32_t strategy, const float* queries,
                          uint64_t qstride, uint32_t nq, uint32_t k, uint32_t l, uint32_t beam,
                          uint32_t* ids, float* dists, dk_search_stats* stats,
-                         cudaStream_t stream);
+                         cudaStream_t stream, const SearchRecord* record = nullptr);

@@ -130,16 +130,14 @@ int32_t plan_warp(dk_index* ix, SearchParams& P, LaunchPlan& L, int mode, double
   // shared-memory budget; the global level takes what a longer search adds.
   P.hash_log2 = 0;
   const uint32_t base = plan_query_smem(P, pq, false);
-  // Per-warp budget (measured on the 1M x 128 workload): the FP32 kernel is fastest with a
-  // shared level holding ~1.1x the mean visited set at load 3/4 (12-20 KB per warp); the
-  // low-precision kernels, capped at 80 registers, with ~9 KB of shared level and more resident
-  // warps; PQ traversal keeps its ADC table and a minimal level.  DK_WARP_SMEM overrides.
+  // Per-warp budget (measured on the 1M x 128 workload): the kernels are fastest with a shared
+  // level holding ~1.1x the mean visited set at load 3/4 (12-20 KB per warp), which keeps
+  // nearly every probe out of the global level, rather than with more resident warps.  PQ
+  // traversal keeps its ADC table and a minimal level.  DK_WARP_SMEM overrides.
   uint32_t dflt = 12288;
-  if (mode == kModeFP32) {
+  if (mode != kModePQ) {
     dflt = base + (uint32_t)(4.0 * est_mean * 1.1 / 0.75);
     dflt = std::min<uint32_t>(std::max<uint32_t>(dflt, 12288), 20480);
-  } else if (mode == kModeBF16 || mode == kModeFP8) {
-    dflt = std::max<uint32_t>(12288, base + 9216);
   }
   const uint32_t budget = std::max<uint32_t>(env_u32("DK_WARP_SMEM", dflt), base + 1024);
   uint32_t slots = align_up((uint32_t)(est_mean * 1.3 / 0.75) + 1, 32);
@@ -191,7 +189,7 @@ int32_t plan_warp(dk_index* ix, SearchParams& P, LaunchPlan& L, int mode, double
 int32_t dk_launch_search(dk_index* ix, int32_t strategy, const float* queries,
                          uint64_t qstride, uint32_t nq, uint32_t k, uint32_t l, uint32_t beam,
                          uint32_t* ids, float* dists, dk_search_stats* stats,
-                         cudaStream_t stream) {
+                         cudaStream_t stream, const SearchRecord* record) {
   if (nq == 0) return DK_OK;
   const int mode = mode_of_strategy(strategy);
   const bool pq = mode == kModePQ;
@@ -204,6 +202,11 @@ int32_t dk_launch_search(dk_index* ix, int32_t strategy, const float* queries,
   P.out_dists = dists;
   P.stats = stats;
   P.hint = ix->hint_dev;
+  if (record) {
+    P.rec_ids = record->ids;
+    P.rec_d = record->dists;
+    P.rec_cap = record->cap;
+  }
   double est = 0, est_mean = 0;
   dk::visited_estimates(ix, P, est, est_mean);
 

@@ -34,6 +34,9 @@ def _lib():
         L.dk_compute_medoid.argtypes = [vp, u64, u32, u32, vp]
         L.dk_build_vamana.restype = i32
         L.dk_build_vamana.argtypes = [vp, u64, u32, u32, u32, i32, ctypes.POINTER(BuildParams), vp, u64, vp]
+        L.dk_build_vamana_device.restype = i32
+        L.dk_build_vamana_device.argtypes = [vp, u64, u32, u32, u32, i32, ctypes.POINTER(BuildParams),
+                                             vp, u64, vp, i32]
         L.dk_pq_train.restype = i32
         L.dk_pq_train.argtypes = [vp, u64, u32, u32, u32, u32, u64, u32, vp, vp]
         L.dk_pq_encode.restype = i32
@@ -66,10 +69,12 @@ def slot_width(pruned_degree: int) -> int:
 
 def build_vamana(base: np.ndarray, metric=Metric.L2, pruned_degree: int = 32, l_build: int = 50,
                  alpha: float = 1.2, max_degree: int | None = None, backedge_ratio: float = 1.0,
-                 num_threads: int = 0, max_batch: int = 0):
+                 num_threads: int = 0, max_batch: int = 0, device: int | None = None):
     """Build a Vamana graph with one frozen start point (a copy of the medoid row, id N).
 
-    Returns ``(vectors, adjacency, degrees, n)`` ready for :class:`GpuProvider`.
+    ``device``: search the larger batches on that CUDA device (``dk_build_vamana_device``; the
+    same graph, faster).  Returns ``(vectors, adjacency, degrees, n)`` ready for
+    :class:`GpuProvider`.
     """
     base = np.ascontiguousarray(base, np.float32)
     n, dim = base.shape
@@ -80,8 +85,14 @@ def build_vamana(base: np.ndarray, metric=Metric.L2, pruned_degree: int = 32, l_
     degrees = np.zeros(n + 1, np.uint32)
     p = BuildParams(pruned_degree, md, l_build, alpha,
                     int(np.ceil(backedge_ratio * pruned_degree)), 0, num_threads, max_batch)
-    _check(_lib().dk_build_vamana(vectors.ctypes.data, dim, n, 1, dim, int(metric), ctypes.byref(p),
-                                  adjacency.ctypes.data, md, degrees.ctypes.data))
+    if device is None:
+        _check(_lib().dk_build_vamana(vectors.ctypes.data, dim, n, 1, dim, int(metric),
+                                      ctypes.byref(p), adjacency.ctypes.data, md,
+                                      degrees.ctypes.data))
+    else:
+        _check(_lib().dk_build_vamana_device(vectors.ctypes.data, dim, n, 1, dim, int(metric),
+                                             ctypes.byref(p), adjacency.ctypes.data, md,
+                                             degrees.ctypes.data, int(device)))
     return vectors, adjacency, degrees, n
 
 

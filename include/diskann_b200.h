@@ -273,6 +273,14 @@ int32_t dk_build_vamana(const float* vectors, uint64_t stride, uint32_t num_poin
                         const dk_build_params* params, uint32_t* adjacency,
                         uint64_t adjacency_stride, uint32_t* degrees);
 
+/* The same build with the greedy searches of every batch of 256 points or more run on CUDA
+ * device `device` (the search kernels of dk_search, bit-exact), pruning and back edges on the
+ * host threads.  Produces exactly the graph dk_build_vamana produces. */
+int32_t dk_build_vamana_device(const float* vectors, uint64_t stride, uint32_t num_points,
+                               uint32_t num_frozen, uint32_t dim, int32_t metric,
+                               const dk_build_params* params, uint32_t* adjacency,
+                               uint64_t adjacency_stride, uint32_t* degrees, int32_t device);
+
 /* Product-quantisation schema: 256 centres per chunk by k-means++ and Lloyd iterations on
  * the given rows; chunk offsets split dim with the first dim % chunks chunks one longer
  * (the reference's FixedChunkPQTable layout, fixed_chunk_pq_table.rs:100-133). */

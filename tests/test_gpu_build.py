@@ -1,0 +1,24 @@
+"""GPU: graph construction with the batch searches on the device (dk_build_vamana_device)
+produces exactly the graph of the host build (dk_build_vamana): the device searches are the
+bit-exact search kernels, so every visited record, prune and back edge is the same."""
+
+import numpy as np
+import pytest
+
+from diskann_b200 import Metric, datasets, graph
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("metric,dim", [(Metric.L2, 64), (Metric.INNER_PRODUCT, 96),
+                                        (Metric.COSINE, 128), (Metric.L2, 384)])
+def test_device_build_equals_host_build(metric, dim):
+    if metric == Metric.L2:
+        base, _ = datasets.gaussian_mixture(6000, dim, 16, 8.0, seed=dim)
+    else:
+        base, _ = datasets.normalized_gaussian(6000, dim, seed=dim)
+    kw = dict(metric=metric, pruned_degree=24, l_build=40, alpha=1.2, max_batch=1024)
+    v0, a0, d0, n0 = graph.build_vamana(base, **kw)
+    v1, a1, d1, n1 = graph.build_vamana(base, device=0, **kw)
+    np.testing.assert_array_equal(d0, d1)
+    np.testing.assert_array_equal(a0, a1)
