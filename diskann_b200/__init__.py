@@ -19,6 +19,7 @@ from .index import (  # noqa: F401
     Metric,
     PQData,
     Quantized,
+    Range,
     STATS_DTYPE,
     SearchServer,
     Status,
@@ -26,5 +27,5 @@ from .index import (  # noqa: F401
 
 __all__ = [
     "ANNError", "BF16", "DiskANNIndex", "FP8", "FullPrecision", "GpuProvider", "Hybrid", "Knn",
-    "KnnSearchError", "Metric", "PQData", "Quantized", "STATS_DTYPE", "SearchServer", "Status",
+    "KnnSearchError", "Metric", "PQData", "Quantized", "Range", "STATS_DTYPE", "SearchServer", "Status",
 ]

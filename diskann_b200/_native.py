@@ -25,6 +25,8 @@ EXPORTED_SYMBOLS = (
     "dk_search",
     "dk_search_device",
     "dk_search_device_noalloc",
+    "dk_range_search",
+    "dk_range_search_device",
     "dk_server_create",
     "dk_server_submit",
     "dk_server_poll",
@@ -134,6 +136,13 @@ def load():
         L.dk_search.argtypes = [vp, i32, vp, u64, u32, u32, u32, u32, vp, vp, vp]
         L.dk_search_device.restype = i32
         L.dk_search_device.argtypes = [vp, i32, vp, u64, u32, u32, u32, u32, vp, vp, vp, vp]
+        f32 = ctypes.c_float
+        L.dk_range_search.restype = i32
+        L.dk_range_search.argtypes = [vp, vp, u64, u32, u32, u32, f32, f32, f32, f32, u32, u32,
+                                      vp, vp, vp]
+        L.dk_range_search_device.restype = i32
+        L.dk_range_search_device.argtypes = [vp, vp, u64, u32, u32, u32, f32, f32, f32, f32, u32,
+                                             u32, vp, vp, vp, vp]
         L.dk_search_device_noalloc.restype = i32
         L.dk_search_device_noalloc.argtypes = [vp, i32, vp, u64, u32, u32, u32, u32, vp, vp, vp, vp]
         L.dk_server_create.restype = i32

@@ -1,0 +1,335 @@
+// Range search (the reference's `Range`, diskann/src/graph/search/range_search.rs) with the
+// FullPrecision accessor, one 128-thread CTA per query, persistent over the batch.
+//
+// Per query: the first round is the batch path's CTA search (cta_search) with a queue of
+// starting_l + F entries and an exact per-CTA bitmap as the visited set; in_range is the first
+// starting_l queue entries with distance <= radius (range_search.rs:179-193); the bitmap is
+// cleared and refilled with them; when |in_range| >= (starting_l as f32 * initial_slack) and
+// |in_range| < max_returned the second round (range_search_internal, range_search.rs:331-389)
+// walks a FIFO frontier - which is in_range itself, in order - popping beam_width nodes,
+// expanding them through the visited set and appending every scored neighbour with distance
+// <= radius * range_slack while |in_range| < max_returned; the post-processor drops start
+// points and keeps inner_radius < distance <= radius, in order.  Stats follow the reference:
+// cmps of the first round; with a second round, hops = first-round hops + (first-round hops
+// + second-round hops) (the scratch counter carries the first round's hops).
+//
+// in_range lives in the caller's output rows (capacity entries per query) and is compacted in
+// place at the end.  With max_returned unlimited the capacity bounds it instead; a query that
+// reaches the capacity then reports flags bit 2 (its results may be incomplete).
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <string>
+
+#include "dk_kernels.cuh"
+
+namespace {
+
+using namespace dk;
+
+struct RangeParams {
+  float radius;
+  float inner_radius;  // NaN: none
+  float initial_slack;
+  float range_slack;
+  uint32_t starting_l;
+  uint32_t max_returned;  // 0: unlimited (bounded by capacity)
+  uint32_t capacity;      // output entries per query
+};
+
+template <int NT, int METRIC, int DIM>
+__global__ void __launch_bounds__(NT) k_range_cta(const SearchParams P, const RangeParams R) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const State S = carve(smem, P);
+  const uint32_t tid = threadIdx.x;
+  Misc* M = S.misc;
+  BitmapSet vset{P.bitmap + (size_t)blockIdx.x * P.bitmap_words, P.bitmap_words};
+  const uint32_t max_ret = R.max_returned ? R.max_returned : R.capacity;
+  const float limit = R.radius * R.range_slack;
+  for (uint32_t qid = blockIdx.x; qid < P.nq; qid += gridDim.x) {
+    uint32_t* out_ids = P.out_ids + (size_t)qid * R.capacity;
+    float* out_d = P.out_dists + (size_t)qid * R.capacity;
+    __syncthreads();
+    uint32_t cmps = 0, hops = 0;
+    cta_search<NT, METRIC, kModeFP32, DIM>(P, S, vset, qid, cmps, hops);
+    __syncthreads();
+    // in_range: the first starting_l queue entries within the radius, in queue order.
+    const float* qd = S.qd[M->cur];
+    const uint32_t* qi = S.qi[M->cur];
+    const uint32_t n_iter = min(M->size, R.starting_l);
+    uint32_t n_in = 0;
+    for (uint32_t i0 = 0; i0 < n_iter; i0 += NT) {
+      const uint32_t i = i0 + tid;
+      const bool in = i < n_iter && qd[i] <= R.radius;
+      uint32_t total;
+      const uint32_t pos = block_scan<NT>(in, M->warp_sums, total);
+      if (in && n_in + pos < max_ret) {
+        out_ids[n_in + pos] = qi[i] & kIdMask;
+        out_d[n_in + pos] = qd[i];
+      }
+      n_in = min(n_in + total, max_ret);
+    }
+    __syncthreads();
+    vset.clear(tid, NT);
+    __syncthreads();
+    for (uint32_t i = tid; i < n_in; i += NT) vset.insert(out_ids[i]);
+    __syncthreads();
+    const bool second = n_in >= (uint32_t)((float)R.starting_l * R.initial_slack) && n_in < max_ret;
+    uint32_t range_hops = 0;
+    if (second) {
+      uint32_t front = 0;
+      while (front < n_in && n_in < max_ret) {
+        const uint32_t nb = min(P.beam, n_in - front);
+        uint32_t count = 0;
+        for (uint32_t b = 0; b < nb; ++b) {
+          const uint32_t* row = P.adj + (size_t)out_ids[front + b] * P.astride;
+          const uint32_t deg = __ldg(row);
+          for (uint32_t t0 = 0; t0 < deg; t0 += NT) {
+            const uint32_t t = t0 + tid;
+            bool fresh = false;
+            uint32_t id = 0;
+            if (t < deg) {
+              id = __ldg(row + 1 + t);
+              fresh = vset.insert(id);
+            }
+            uint32_t total;
+            const uint32_t pos = block_scan<NT>(fresh, M->warp_sums, total);
+            if (fresh) S.cand_id[count + pos] = id;
+            count += total;
+          }
+        }
+        front += nb;
+        __syncthreads();
+        cta_score<NT, METRIC, kModeFP32, DIM>(P, S, S.cand_id, S.cand_d, count);
+        __syncthreads();
+        // Append, in expansion order, the neighbours within radius * range_slack while room.
+        for (uint32_t i0 = 0; i0 < count; i0 += NT) {
+          const uint32_t i = i0 + tid;
+          const bool in = i < count && S.cand_d[i] <= limit;
+          uint32_t total;
+          const uint32_t pos = block_scan<NT>(in, M->warp_sums, total);
+          if (in && n_in + pos < max_ret) {
+            out_ids[n_in + pos] = S.cand_id[i];
+            out_d[n_in + pos] = S.cand_d[i];
+          }
+          n_in = min(n_in + total, max_ret);
+        }
+        range_hops += nb;
+        __syncthreads();
+      }
+    }
+    // Post-process: FilterStartPoints, then inner_radius < distance <= radius, in order,
+    // compacted in place (every element of a chunk is read before the chunk's writes).
+    uint32_t written = 0;
+    for (uint32_t i0 = 0; i0 < n_in; i0 += NT) {
+      const uint32_t i = i0 + tid;
+      uint32_t id = 0;
+      float d = 0.0f;
+      bool keep = false;
+      if (i < n_in) {
+        id = out_ids[i];
+        d = out_d[i];
+        keep = id < P.n && d <= R.radius && !(R.inner_radius == R.inner_radius && d <= R.inner_radius);
+      }
+      uint32_t total;
+      const uint32_t pos = block_scan<NT>(keep, M->warp_sums, total);
+      if (keep) {
+        out_ids[written + pos] = id;
+        out_d[written + pos] = d;
+      }
+      written += total;
+      __syncthreads();
+    }
+    for (uint32_t j = written + tid; j < R.capacity; j += NT) {
+      out_ids[j] = DK_INVALID_ID;
+      out_d[j] = INFINITY;
+    }
+    if (tid == 0) {
+      const bool truncated = R.max_returned == 0 && n_in >= R.capacity;
+      P.stats[qid] = dk_search_stats{cmps, second ? hops + hops + range_hops : hops, written,
+                                     (second ? 2u : 0u) | (truncated ? 4u : 0u)};
+    }
+  }
+}
+
+template <int METRIC, int DIM>
+cudaError_t launch_range(const SearchParams& P, const RangeParams& R, uint32_t grid,
+                         cudaStream_t stream) {
+  auto k = k_range_cta<kCtaThreads, METRIC, DIM>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P.smem_bytes);
+  if (e != cudaSuccess) return e;
+  k<<<grid, kCtaThreads, P.smem_bytes, stream>>>(P, R);
+  return cudaGetLastError();
+}
+
+template <int METRIC>
+cudaError_t range_dims(const SearchParams& P, const RangeParams& R, uint32_t grid,
+                       cudaStream_t stream) {
+  switch (P.dim) {
+    case 96: return launch_range<METRIC, 96>(P, R, grid, stream);
+    case 128: return launch_range<METRIC, 128>(P, R, grid, stream);
+    case 384: return launch_range<METRIC, 384>(P, R, grid, stream);
+    case 768: return launch_range<METRIC, 768>(P, R, grid, stream);
+    default: return launch_range<METRIC, 0>(P, R, grid, stream);
+  }
+}
+
+int32_t fail(int32_t status, const std::string& msg) {
+  dk_set_error(status, msg);
+  return status;
+}
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int now = -1;
+    cudaGetDevice(&now);
+    if (prev >= 0 && now != prev) cudaSetDevice(prev);
+  }
+};
+
+// Range::with_options validation (range_search.rs:63-110) plus this API's own bounds.
+int32_t check_range(const dk_index* ix, uint32_t starting_l, uint32_t beam_width, float radius,
+                    float inner_radius, float initial_slack, float range_slack,
+                    uint32_t max_returned, uint32_t capacity, uint64_t qstride) {
+  if (!ix) return fail(DK_ERR_INVALID_ARGUMENT, "index is null");
+  if (beam_width == 0) return fail(DK_ERR_BEAM_WIDTH_ZERO, "beam width cannot be zero");
+  if (starting_l == 0) return fail(DK_ERR_L_ZERO, "l_value cannot be zero");
+  if (max_returned && max_returned < starting_l)
+    return fail(DK_ERR_INVALID_ARGUMENT, "max_returned must be greater than or equal to starting_l");
+  if (!(initial_slack >= 0.0f && initial_slack <= 1.0f))
+    return fail(DK_ERR_INVALID_ARGUMENT, "initial_search_slack must be between 0 and 1.0");
+  if (!(range_slack >= 1.0f))
+    return fail(DK_ERR_INVALID_ARGUMENT, "range_search_slack must be greater than or equal to 1.0");
+  if (!std::isnan(inner_radius) && inner_radius > radius)
+    return fail(DK_ERR_INVALID_ARGUMENT, "inner_radius must be less than or equal to radius");
+  if (capacity < starting_l) return fail(DK_ERR_INVALID_ARGUMENT, "capacity below starting_l");
+  if (max_returned && capacity < max_returned)
+    return fail(DK_ERR_INVALID_ARGUMENT, "capacity below max_returned");
+  if (beam_width > 64) return fail(DK_ERR_UNSUPPORTED, "beam_width above 64 is not supported");
+  if ((uint64_t)starting_l + ix->f > 16384) return fail(DK_ERR_UNSUPPORTED, "starting_l above 16383 is not supported");
+  if (qstride < ix->dim) return fail(DK_ERR_DIMENSION_MISMATCH, "query stride below dim");
+  return DK_OK;
+}
+
+int32_t launch_range_search(dk_index* ix, const float* queries, uint64_t qstride, uint32_t nq,
+                            const RangeParams& R, uint32_t beam, uint32_t* ids, float* dists,
+                            dk_search_stats* stats, cudaStream_t stream) {
+  if (nq == 0) return DK_OK;
+  SearchParams P{};
+  dk::base_params(ix, DK_STRATEGY_FULL_PRECISION, 1, R.starting_l, beam, P);
+  P.queries = queries;
+  P.qstride = qstride;
+  P.nq = nq;
+  P.out_ids = ids;
+  P.out_dists = dists;
+  P.stats = stats;
+  P.hash_limit = 0xFFFFFFFFu;  // the bitmap never fills
+  P.smem_bytes = dk::plan_query_smem(P, false, false);
+  int max_optin = 0, sms = 0;
+  cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ix->device);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ix->device);
+  if (P.smem_bytes > (uint32_t)max_optin)
+    return fail(DK_ERR_UNSUPPORTED, "search state does not fit in shared memory (starting_l too large)");
+  // One exact bitmap over all ids per CTA; up to two CTAs per SM, within 512 MiB.
+  const uint32_t words = (ix->n + ix->f + 31u) / 32u;
+  const uint64_t per = (uint64_t)words * 4u;
+  uint32_t grid = std::min<uint32_t>(nq, 2u * (uint32_t)std::max(1, sms));
+  if (per * grid > (512ull << 20)) grid = (uint32_t)std::max<uint64_t>(1, (512ull << 20) / per);
+  unsigned char* scratch = nullptr;
+  cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&scratch), per * grid, ix->pool, stream);
+  if (e != cudaSuccess)
+    return fail(DK_ERR_OUT_OF_MEMORY, std::string("range scratch: ") + cudaGetErrorString(e));
+  P.bitmap = reinterpret_cast<uint32_t*>(scratch);
+  P.bitmap_words = words;
+  switch (ix->metric) {
+    case DK_METRIC_L2: e = range_dims<DK_METRIC_L2>(P, R, grid, stream); break;
+    case DK_METRIC_INNER_PRODUCT: e = range_dims<DK_METRIC_INNER_PRODUCT>(P, R, grid, stream); break;
+    case DK_METRIC_COSINE: e = range_dims<DK_METRIC_COSINE>(P, R, grid, stream); break;
+    default: e = range_dims<DK_METRIC_COSINE_NORMALIZED>(P, R, grid, stream); break;
+  }
+  cudaFreeAsync(scratch, stream);
+  if (e != cudaSuccess) return fail(DK_ERR_CUDA, std::string("range launch: ") + cudaGetErrorString(e));
+  return DK_OK;
+}
+
+}  // namespace
+
+extern "C" int32_t dk_range_search_device(dk_index* ix, const float* queries,
+                                          uint64_t query_stride, uint32_t nq, uint32_t starting_l,
+                                          uint32_t beam_width, float radius, float inner_radius,
+                                          float initial_slack, float range_slack,
+                                          uint32_t max_returned, uint32_t capacity, uint32_t* ids,
+                                          float* dists, dk_search_stats* stats, void* stream) {
+  const int32_t v = check_range(ix, starting_l, beam_width, radius, inner_radius, initial_slack,
+                                range_slack, max_returned, capacity, query_stride);
+  if (v != DK_OK) return v;
+  if (nq && (!queries || !ids || !dists || !stats))
+    return fail(DK_ERR_INVALID_ARGUMENT, "queries, ids, dists and stats are required");
+  DeviceGuard guard(ix->device);
+  const RangeParams R{radius, inner_radius, initial_slack, range_slack, starting_l, max_returned,
+                      capacity};
+  return launch_range_search(ix, queries, query_stride, nq, R, beam_width, ids, dists, stats,
+                             static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int32_t dk_range_search(dk_index* ix, const float* queries, uint64_t query_stride,
+                                   uint32_t nq, uint32_t starting_l, uint32_t beam_width,
+                                   float radius, float inner_radius, float initial_slack,
+                                   float range_slack, uint32_t max_returned, uint32_t capacity,
+                                   uint32_t* ids, float* dists, dk_search_stats* stats) {
+  const int32_t v = check_range(ix, starting_l, beam_width, radius, inner_radius, initial_slack,
+                                range_slack, max_returned, capacity, query_stride);
+  if (v != DK_OK) return v;
+  if (nq == 0) return DK_OK;
+  if (!queries || !ids || !dists) return fail(DK_ERR_INVALID_ARGUMENT, "queries, ids and dists are required");
+  DeviceGuard guard(ix->device);
+  cudaStream_t s = nullptr;
+  cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return fail(DK_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
+  const size_t qbytes = (size_t)nq * ix->dim * 4, obytes = (size_t)nq * capacity * 4;
+  const size_t off_ids = (qbytes + 255) / 256 * 256;
+  const size_t off_d = off_ids + (obytes + 255) / 256 * 256;
+  const size_t off_st = off_d + (obytes + 255) / 256 * 256;
+  const size_t total = off_st + (size_t)nq * sizeof(dk_search_stats);
+  unsigned char* buf = nullptr;
+  e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&buf), total, ix->pool, s);
+  if (e != cudaSuccess) {
+    cudaStreamDestroy(s);
+    return fail(DK_ERR_OUT_OF_MEMORY, std::string("range buffers: ") + cudaGetErrorString(e));
+  }
+  if (query_stride == ix->dim)
+    e = cudaMemcpyAsync(buf, queries, qbytes, cudaMemcpyHostToDevice, s);
+  else
+    e = cudaMemcpy2DAsync(buf, ix->dim * 4, queries, query_stride * 4, ix->dim * 4, nq,
+                          cudaMemcpyHostToDevice, s);
+  int32_t rc = DK_OK;
+  if (e == cudaSuccess) {
+    const RangeParams R{radius, inner_radius, initial_slack, range_slack, starting_l,
+                        max_returned, capacity};
+    rc = launch_range_search(ix, reinterpret_cast<const float*>(buf), ix->dim, nq, R, beam_width,
+                             reinterpret_cast<uint32_t*>(buf + off_ids),
+                             reinterpret_cast<float*>(buf + off_d),
+                             reinterpret_cast<dk_search_stats*>(buf + off_st), s);
+    if (rc == DK_OK) {
+      e = cudaMemcpyAsync(ids, buf + off_ids, obytes, cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(dists, buf + off_d, obytes, cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess && stats)
+        e = cudaMemcpyAsync(stats, buf + off_st, (size_t)nq * sizeof(dk_search_stats), cudaMemcpyDeviceToHost, s);
+    }
+  }
+  cudaFreeAsync(buf, s);
+  const cudaError_t es = cudaStreamSynchronize(s);
+  cudaStreamDestroy(s);
+  if (rc != DK_OK) return rc;
+  if (e != cudaSuccess) return fail(DK_ERR_CUDA, std::string("range copy: ") + cudaGetErrorString(e));
+  if (es != cudaSuccess) return fail(DK_ERR_CUDA, std::string("range search: ") + cudaGetErrorString(es));
+  return DK_OK;
+}

@@ -101,6 +101,38 @@ class Knn:
         return f"Knn(k={self.k_value}, l={self.l_value}, beam_width={self.beam_width})"
 
 
+class Range:
+    """Range search parameters (range_search.rs:63-110): ``Range(starting_l, radius,
+    beam_width=None, inner_radius=None, initial_slack=1.0, range_slack=1.0,
+    max_returned=None)``."""
+
+    def __init__(self, starting_l: int, radius: float, beam_width: int | None = None,
+                 inner_radius: float | None = None, initial_slack: float = 1.0,
+                 range_slack: float = 1.0, max_returned: int | None = None):
+        bw = 1 if beam_width is None else int(beam_width)
+        if bw == 0:
+            raise KnnSearchError(Status.BEAM_WIDTH_ZERO, "beam width cannot be zero")
+        if starting_l == 0:
+            raise KnnSearchError(Status.L_ZERO, "l_value cannot be zero")
+        if max_returned is not None and max_returned < starting_l:
+            raise ANNError(Status.INVALID_ARGUMENT,
+                           "max_returned must be greater than or equal to starting_l")
+        if not 0.0 <= initial_slack <= 1.0:
+            raise ANNError(Status.INVALID_ARGUMENT, "initial_search_slack must be between 0 and 1.0")
+        if range_slack < 1.0:
+            raise ANNError(Status.INVALID_ARGUMENT,
+                           "range_search_slack must be greater than or equal to 1.0")
+        if inner_radius is not None and inner_radius > radius:
+            raise ANNError(Status.INVALID_ARGUMENT, "inner_radius must be less than or equal to radius")
+        self.starting_l = int(starting_l)
+        self.radius = float(radius)
+        self.beam_width = bw
+        self.inner_radius = inner_radius
+        self.initial_slack = float(initial_slack)
+        self.range_slack = float(range_slack)
+        self.max_returned = max_returned
+
+
 class _Strategy:
     code = -1
 
@@ -246,6 +278,29 @@ class DiskANNIndex:
             params.l_value, params.beam_width, ids.ctypes.data, dists.ctypes.data, stats.ctypes.data,
         ))
         return ids, dists, stats
+
+    def range_search(self, params: Range, queries, capacity: int | None = None):
+        """Range search of host queries (FullPrecision, ``dk_range_search``).  Returns
+        ``(results, stats)``: per query a ``(ids, dists)`` pair of its results, and the stats
+        array (flags bit 1: second round ran; bit 2: results reached the capacity)."""
+        q = np.ascontiguousarray(np.atleast_2d(queries), dtype=np.float32)
+        if q.shape[1] != self.provider.dim:
+            raise ANNError(Status.DIMENSION_MISMATCH, f"query dim {q.shape[1]} != {self.provider.dim}")
+        cap = capacity or params.max_returned or self.provider.num_points
+        cap = max(cap, params.starting_l, params.max_returned or 0)
+        nq = q.shape[0]
+        ids = np.empty((nq, cap), dtype=np.uint32)
+        dists = np.empty((nq, cap), dtype=np.float32)
+        stats = np.zeros(nq, dtype=STATS_DTYPE)
+        _check(_native.load().dk_range_search(
+            self.provider.handle, q.ctypes.data, q.shape[1], nq, params.starting_l,
+            params.beam_width, params.radius,
+            float("nan") if params.inner_radius is None else params.inner_radius,
+            params.initial_slack, params.range_slack, params.max_returned or 0, cap,
+            ids.ctypes.data, dists.ctypes.data, stats.ctypes.data))
+        out = [(ids[i, : stats[i]["result_count"]], dists[i, : stats[i]["result_count"]])
+               for i in range(nq)]
+        return out, stats
 
     def search_device(self, params: Knn, strategy: _Strategy, queries, ids, dists, stats,
                       stream=None) -> None:

@@ -160,6 +160,30 @@ int32_t dk_search_device(dk_index* index, int32_t strategy, const float* queries
                          uint32_t beam_width, uint32_t* ids, float* dists,
                          dk_search_stats* stats, void* stream);
 
+/* Range search with the FullPrecision strategy (replaces DiskANNIndex::search with the
+ * reference's `Range` parameters, diskann/src/graph/search/range_search.rs:63-389): a first
+ * greedy search with a queue of starting_l + F entries, then - when at least
+ * (starting_l * initial_slack) of its first starting_l entries lie within `radius` and fewer
+ * than max_returned - a breadth-first second round from them that adds every neighbour within
+ * radius * range_slack; results are the start-point-free entries with
+ * inner_radius < distance <= radius, in the reference's order.  inner_radius NaN = none;
+ * max_returned 0 = unlimited.  Each query gets `capacity` (>= starting_l, >= max_returned) output
+ * slots: result_count in stats says how many are filled; with max_returned unlimited, flags
+ * bit 2 marks a query whose results reached the capacity (possibly incomplete); flags bit 1:
+ * the second round ran.  Stats follow the reference (cmps of the first round; with a second
+ * round, hops counts the first round twice, as the reference's scratch counter does). */
+int32_t dk_range_search(dk_index* index, const float* queries, uint64_t query_stride,
+                        uint32_t nq, uint32_t starting_l, uint32_t beam_width, float radius,
+                        float inner_radius, float initial_slack, float range_slack,
+                        uint32_t max_returned, uint32_t capacity, uint32_t* ids, float* dists,
+                        dk_search_stats* stats);
+/* The same with device buffers, asynchronous on `stream`; `stats` is required. */
+int32_t dk_range_search_device(dk_index* index, const float* queries, uint64_t query_stride,
+                               uint32_t nq, uint32_t starting_l, uint32_t beam_width,
+                               float radius, float inner_radius, float initial_slack,
+                               float range_slack, uint32_t max_returned, uint32_t capacity,
+                               uint32_t* ids, float* dists, dk_search_stats* stats, void* stream);
+
 /* Same search, arguments and results as dk_search_device, for callers that cannot allocate
  * device memory while they search: for example a process whose own caching allocator took the
  * GPU's free memory at start-up (so the allocation inside dk_search_device would fail), or a

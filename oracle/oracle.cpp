@@ -22,6 +22,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <deque>
 #include <thread>
 #include <unordered_set>
 #include <vector>
@@ -248,6 +249,10 @@ struct VisitedSet {
   }
   static size_t hash(uint32_t id) { return (size_t)(id * 2654435761u); }
   // Returns true if `id` was newly inserted.
+  void clear() {
+    std::fill(slots.begin(), slots.end(), 0xFFFFFFFFu);
+    count = 0;
+  }
   bool insert(uint32_t id) {
     if (2 * (count + 1) > slots.size()) grow();
     size_t h = hash(id) & mask;
@@ -341,6 +346,40 @@ struct Scorer {
   }
 };
 
+// One node of `expand_beam`: its adjacency list in stored order, retained by the visited-set
+// insert predicate (glue.rs:524-561 NotInMut), each retained id scored, in order.
+template <class Score>
+void expand(const orc_index* ix, const Score& score, VisitedSet& visited, uint32_t node,
+            std::vector<std::pair<uint32_t, float>>& out) {
+  const uint32_t deg = ix->degrees[node];
+  const uint32_t* adj = ix->adjacency + (size_t)node * ix->adjacency_stride;
+  for (uint32_t t = 0; t < deg; ++t) {
+    const uint32_t id = adj[t];
+    if (visited.insert(id)) out.emplace_back(id, score(id));
+  }
+}
+
+// The `search_internal` loop after the start points (index.rs:1964-2005).
+template <class Score>
+void search_loop(const orc_index* ix, const Score& score, Queue& best, VisitedSet& visited,
+                 uint32_t beam_width, uint32_t& cmps, uint32_t& hops) {
+  std::vector<uint32_t> beam;
+  std::vector<std::pair<uint32_t, float>> neighbors;
+  neighbors.reserve((size_t)ix->max_degree * beam_width);
+  while (best.has_notvisited()) {
+    beam.clear();
+    uint32_t node;
+    while (beam.size() < beam_width && best.closest_notvisited(&node)) beam.push_back(node);
+    neighbors.clear();
+    // expand_beam: per beam node, its adjacency list in stored order, retained by the
+    // visited-set insert predicate (glue.rs:524-561 NotInMut), scored in order.
+    for (uint32_t n : beam) expand(ix, score, visited, n, neighbors);
+    for (const auto& nb : neighbors) best.insert(nb.first, nb.second);
+    cmps += (uint32_t)neighbors.size();
+    hops += (uint32_t)beam.size();
+  }
+}
+
 }  // namespace
 
 // diskann/src/graph/search/knn_search.rs:94-119 `Knn::new` validation.
@@ -349,6 +388,102 @@ extern "C" int32_t orc_validate_knn(uint32_t k, uint32_t l, uint32_t beam_width)
   if (l == 0) return ORC_ERR_L_ZERO;
   if (k > l) return ORC_ERR_L_LESS_THAN_K;
   if (beam_width == 0) return ORC_ERR_BEAM_WIDTH_ZERO;
+  return ORC_OK;
+}
+
+// Range search (diskann/src/graph/search/range_search.rs), FullPrecision accessor:
+//   Range::with_options validation (range_search.rs:63-110);
+//   `search` (range_search.rs:157-247): search_internal with a queue of starting_l + #start
+//     points; in_range = the first starting_l queue entries with distance <= radius; the
+//     visited set is cleared and refilled with them; a second round runs when
+//     |in_range| >= (starting_l as f32 * initial_slack) as usize and |in_range| < max_returned;
+//     the post-processor (FilterStartPoints + copy) writes in_range through DistanceFiltered
+//     (inner_radius < distance <= radius);
+//   `range_search_internal` (range_search.rs:331-389): a FIFO frontier seeded with in_range;
+//     pop beam_width nodes, expand them through the visited set, append every scored neighbour
+//     with distance <= radius * range_slack while |in_range| < max_returned.
+//   Stats: cmps of the first round only; when the second round runs, hops = the first round's
+//     hops plus the scratch counter, which itself started at the first round's hops
+//     (range_search.rs:204-209, 380-387), so the first round's hops count twice.
+// inner_radius NaN means none; max_returned 0 means unlimited; at most `capacity` results are
+// written (flags bit 2 set if more passed the filter).  flags bit 1: second round ran.
+extern "C" int32_t orc_range_search(const orc_index* ix, const float* query, uint32_t starting_l,
+                                    uint32_t beam_width, float radius, float inner_radius,
+                                    float initial_slack, float range_slack, uint32_t max_returned,
+                                    uint32_t capacity, uint32_t* ids_out, float* dists_out,
+                                    orc_stats* stats) {
+  if (beam_width == 0) return ORC_ERR_BEAM_WIDTH_ZERO;
+  if (starting_l == 0) return ORC_ERR_L_ZERO;
+  if (max_returned && max_returned < starting_l) return ORC_ERR_INVALID_ARGUMENT;
+  if (!(initial_slack >= 0.0f && initial_slack <= 1.0f)) return ORC_ERR_INVALID_ARGUMENT;
+  if (!(range_slack >= 1.0f)) return ORC_ERR_INVALID_ARGUMENT;
+  if (!std::isnan(inner_radius) && inner_radius > radius) return ORC_ERR_INVALID_ARGUMENT;
+  const size_t max_ret = max_returned ? max_returned : SIZE_MAX;
+
+  Scorer score{ix, query, false, {}};
+  const uint32_t n_start = ix->num_frozen;
+  Queue best((size_t)starting_l + n_start);
+  VisitedSet visited((size_t)std::ceil(1.1 * ix->max_degree * 1.3 * starting_l));
+  uint32_t cmps = 0, hops = 0;
+  for (uint32_t s = 0; s < n_start; ++s) {
+    const uint32_t id = ix->num_points + s;
+    visited.insert(id);
+    best.insert(id, score(id));
+    cmps += 1;
+  }
+  search_loop(ix, score, best, visited, beam_width, cmps, hops);
+
+  std::vector<std::pair<uint32_t, float>> in_range;
+  const size_t n_iter = std::min(best.iter_len(), (size_t)starting_l);
+  for (size_t i = 0; i < n_iter; ++i)
+    if (best.dists[i] <= radius) in_range.emplace_back(best.ids[i], best.dists[i]);
+  visited.clear();
+  for (const auto& e : in_range) visited.insert(e.first);
+  const bool second = in_range.size() >= (size_t)((float)starting_l * initial_slack) &&
+                      in_range.size() < max_ret;
+  uint32_t total_hops = hops;
+  if (second) {
+    std::deque<uint32_t> frontier;
+    for (const auto& e : in_range) frontier.push_back(e.first);
+    const float limit = radius * range_slack;
+    uint32_t scratch_hops = hops;
+    std::vector<uint32_t> beam;
+    std::vector<std::pair<uint32_t, float>> neighbors;
+    while (!frontier.empty() && in_range.size() < max_ret) {
+      beam.clear();
+      while (!frontier.empty() && beam.size() < beam_width) {
+        beam.push_back(frontier.front());
+        frontier.pop_front();
+      }
+      neighbors.clear();
+      for (uint32_t n : beam) expand(ix, score, visited, n, neighbors);
+      for (const auto& nb : neighbors)
+        if (nb.second <= limit && in_range.size() < max_ret) {
+          in_range.push_back(nb);
+          frontier.push_back(nb.first);
+        }
+      scratch_hops += (uint32_t)beam.size();
+    }
+    total_hops = hops + scratch_hops;
+  }
+  uint32_t count = 0, passed = 0;
+  for (const auto& e : in_range) {
+    if (e.first >= ix->num_points) continue;  // FilterStartPoints
+    if (!std::isnan(inner_radius) && e.second <= inner_radius) continue;
+    if (!(e.second <= radius)) continue;
+    ++passed;
+    if (count < capacity) {
+      ids_out[count] = e.first;
+      dists_out[count] = e.second;
+      ++count;
+    }
+  }
+  if (stats) {
+    stats->cmps = cmps;
+    stats->hops = total_hops;
+    stats->result_count = count;
+    stats->flags = (second ? 2u : 0u) | (passed > count ? 4u : 0u);
+  }
   return ORC_OK;
 }
 
@@ -393,28 +528,7 @@ extern "C" int32_t orc_search(const orc_index* ix, int32_t strategy, const float
     cmps += 1;
   }
 
-  std::vector<uint32_t> beam;
-  std::vector<std::pair<uint32_t, float>> neighbors;
-  neighbors.reserve((size_t)ix->max_degree * beam_width);
-  while (best.has_notvisited()) {
-    beam.clear();
-    uint32_t node;
-    while (beam.size() < beam_width && best.closest_notvisited(&node)) beam.push_back(node);
-    neighbors.clear();
-    // expand_beam: per beam node, its adjacency list in stored order, retained by the
-    // visited-set insert predicate (glue.rs:524-561 NotInMut), scored in order.
-    for (uint32_t n : beam) {
-      const uint32_t deg = ix->degrees[n];
-      const uint32_t* adj = ix->adjacency + (size_t)n * ix->adjacency_stride;
-      for (uint32_t t = 0; t < deg; ++t) {
-        const uint32_t id = adj[t];
-        if (visited.insert(id)) neighbors.emplace_back(id, score(id));
-      }
-    }
-    for (const auto& nb : neighbors) best.insert(nb.first, nb.second);
-    cmps += (uint32_t)neighbors.size();
-    hops += (uint32_t)beam.size();
-  }
+  search_loop(ix, score, best, visited, beam_width, cmps, hops);
 
   // Post-processing over the first min(search_l, size) candidates.
   const size_t n_cand = best.iter_len();

@@ -28,6 +28,7 @@ enum {
   ORC_ERR_L_LESS_THAN_K = 3,
   ORC_ERR_BEAM_WIDTH_ZERO = 4,
   ORC_ERR_NO_PQ = 5,
+  ORC_ERR_INVALID_ARGUMENT = 6,
 };
 
 #define ORC_INVALID_ID 0xFFFFFFFFu
@@ -64,6 +65,10 @@ int32_t orc_validate_knn(uint32_t k, uint32_t l, uint32_t beam_width);
 int32_t orc_search(const orc_index* ix, int32_t strategy, const float* query, uint32_t k,
                    uint32_t l, uint32_t beam_width, uint32_t* ids_out, float* dists_out,
                    orc_stats* stats);
+int32_t orc_range_search(const orc_index* ix, const float* query, uint32_t starting_l,
+                         uint32_t beam_width, float radius, float inner_radius,
+                         float initial_slack, float range_slack, uint32_t max_returned,
+                         uint32_t capacity, uint32_t* ids_out, float* dists_out, orc_stats* stats);
 int32_t orc_search_batch(const orc_index* ix, int32_t strategy, const float* queries,
                          uint32_t query_stride, uint32_t nq, uint32_t k, uint32_t l,
                          uint32_t beam_width, uint32_t* ids_out, float* dists_out,

@@ -101,6 +101,11 @@ def lib():
             ]
             L.orc_pq_table.restype = None
             L.orc_pq_table.argtypes = [ctypes.POINTER(_Index), ctypes.c_void_p, ctypes.c_void_p]
+            L.orc_range_search.restype = ctypes.c_int32
+            L.orc_range_search.argtypes = [
+                ctypes.POINTER(_Index), ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32,
+                ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_uint32,
+                ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
             _lib = L
     return _lib
 
@@ -169,6 +174,24 @@ class OracleIndex:
         if rc != 0:
             raise ValueError(f"oracle search failed with status {rc}")
         return ids, dists, stats
+
+    def range_search(self, query, starting_l, radius, beam_width=1, inner_radius=None,
+                     initial_slack=1.0, range_slack=1.0, max_returned=0, capacity=None):
+        """Range search of one query (range_search.rs restated); returns ``(ids, dists, stats)``
+        with the results that passed the filter (stats["flags"] bit 1: second round ran)."""
+        q = np.ascontiguousarray(np.ravel(query), dtype=np.float32)
+        cap = capacity if capacity is not None else (max_returned or self.num_points)
+        ids = np.empty(max(cap, 1), dtype=np.uint32)
+        dists = np.empty(max(cap, 1), dtype=np.float32)
+        st = np.zeros(1, dtype=STATS_DTYPE)
+        rc = lib().orc_range_search(
+            ctypes.byref(self._s), _ptr(q), starting_l, beam_width, radius,
+            float("nan") if inner_radius is None else inner_radius, initial_slack, range_slack,
+            max_returned, cap, _ptr(ids), _ptr(dists), _ptr(st))
+        if rc != 0:
+            raise ValueError(f"oracle range search failed with status {rc}")
+        n = int(st[0]["result_count"])
+        return ids[:n], dists[:n], st[0]
 
     def pq_table(self, query):
         q = np.ascontiguousarray(query, dtype=np.float32)

@@ -10,7 +10,9 @@ tests compare.  Run it from the repository root:
 
     python tests/golden/make_golden.py /path/to/reference
 
-It writes ``tests/golden/grid_search.json`` and ``tests/golden/flat_knn_search.json``.
+It writes ``tests/golden/grid_search.json``, ``tests/golden/flat_knn_search.json`` and
+``tests/golden/range_search.json`` (range_search.rs's baselines with the Range parameters of
+each case).
 """
 
 import json
@@ -18,6 +20,16 @@ import os
 import sys
 
 GRID_DIR = "diskann/test/generated/graph/test/cases/grid_search"
+RANGE_DIR = "diskann/test/generated/graph/test/cases/range_search"
+# Range parameters of each case (diskann/src/graph/test/cases/range_search.rs): 3-D grid of
+# size 5, default query, beam width 1; (max_returned or None, initial_slack, range_slack).
+RANGE_CASES = {
+    "basic_range_search.json": (None, 1.0, 1.0),
+    "inner_radius_filtering.json": (None, 1.0, 1.0),
+    "two_round_search.json": (None, 1.0, 1.0),
+    "max_results_respected_means_no_second_round.json": (4, 1.0, 1.0),
+    "max_results_respected_and_second_round_triggered.json": (5, 1.0, 1.0),
+}
 FLAT_DIR = "diskann/test/generated/flat/test/cases/flat_knn_search"
 GRID_FILES = ["search_1_100.json", "search_3_5.json", "search_4_4.json"]
 FLAT_FILES = ["search_1_100.json", "search_2_5.json", "search_3_4.json"]
@@ -67,7 +79,33 @@ def main(ref_root: str) -> None:
             )
     with open(os.path.join(out_dir, "flat_knn_search.json"), "w") as f:
         json.dump(flat, f, indent=1)
-    print(f"wrote {len(grid)} grid cases and {len(flat)} flat cases to {out_dir}")
+
+    rng = []
+    for name, (max_returned, initial_slack, range_slack) in RANGE_CASES.items():
+        with open(os.path.join(ref_root, RANGE_DIR, name)) as f:
+            c = json.load(f)["payload"]
+        rng.append(
+            {
+                "source": f"{RANGE_DIR}/{name}",
+                "grid_dims": 3,
+                "grid_size": c["grid_size"],
+                "query": c["query"],
+                "radius": c["radius"],
+                "inner_radius": c["inner_radius"],
+                "starting_l": c["starting_l"],
+                "max_returned": max_returned,
+                "initial_slack": initial_slack,
+                "range_slack": range_slack,
+                "results": c["results"],
+                "comparisons": c["comparisons"],
+                "hops": c["hops"],
+                "result_count": c["result_count"],
+                "second_round": c["range_search_second_round"],
+            }
+        )
+    with open(os.path.join(out_dir, "range_search.json"), "w") as f:
+        json.dump(rng, f, indent=1)
+    print(f"wrote {len(grid)} grid, {len(flat)} flat and {len(rng)} range cases to {out_dir}")
 
 
 if __name__ == "__main__":

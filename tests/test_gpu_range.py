@@ -1,0 +1,85 @@
+"""GPU: range search (dk_range_search, the reference's `Range`) against range_search.rs's
+golden baselines and the oracle, bit for bit: result ids and distances in order, comparison
+and hop counts, result count and the second-round flag."""
+
+import json
+import os
+
+import numpy as np
+import pytest
+
+from diskann_b200 import (ANNError, DiskANNIndex, GpuProvider, KnnSearchError, Metric, Range,
+                          Status, datasets)
+from oracle import oracle as O
+from tests.helpers import queries_like, random_index
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _cases():
+    with open(os.path.join(GOLDEN, "range_search.json")) as f:
+        return json.load(f)
+
+
+@pytest.mark.parametrize("case", _cases(), ids=lambda c: c["source"].split("/")[-1][:-5])
+def test_range_golden_through_abi(case):
+    v, a, d, n = datasets.grid(case["grid_dims"], case["grid_size"])
+    idx = DiskANNIndex(GpuProvider(v, a, d, n, Metric.L2))
+    params = Range(case["starting_l"], case["radius"], inner_radius=case["inner_radius"],
+                   initial_slack=case["initial_slack"], range_slack=case["range_slack"],
+                   max_returned=case["max_returned"])
+    res, st = idx.range_search(params, np.array(case["query"], np.float32))
+    ids, dists = res[0]
+    assert [[int(i), float(x)] for i, x in zip(ids, dists)] == case["results"]
+    assert int(st[0]["cmps"]) == case["comparisons"]
+    assert int(st[0]["hops"]) == case["hops"]
+    assert int(st[0]["result_count"]) == case["result_count"]
+    assert bool(int(st[0]["flags"]) & 2) == case["second_round"]
+
+
+def _assert_same(idx, orc, q, p, capacity=None):
+    res, st = idx.range_search(p, q, capacity=capacity)
+    for i in range(q.shape[0]):
+        oi, od, os_ = orc.range_search(q[i], p.starting_l, p.radius, beam_width=p.beam_width,
+                                       inner_radius=p.inner_radius, initial_slack=p.initial_slack,
+                                       range_slack=p.range_slack, max_returned=p.max_returned or 0,
+                                       capacity=capacity)
+        np.testing.assert_array_equal(res[i][0], oi)
+        np.testing.assert_array_equal(res[i][1].view(np.uint32), od.view(np.uint32))
+        assert int(st[i]["cmps"]) == int(os_["cmps"]) and int(st[i]["hops"]) == int(os_["hops"])
+        assert int(st[i]["flags"]) & 2 == int(os_["flags"]) & 2
+
+
+@pytest.mark.parametrize("metric", [Metric.L2, Metric.INNER_PRODUCT, Metric.COSINE])
+@pytest.mark.parametrize("dim", [64, 128])
+def test_range_parity_with_the_oracle(metric, dim):
+    norm = metric != Metric.L2
+    v, a, d, n = random_index(3000, dim, 24, seed=dim + int(metric), metric=int(metric),
+                              normalize=norm, max_degree=31)
+    q = queries_like(v[:n], 16, seed=5, normalize=norm)
+    idx = DiskANNIndex(GpuProvider(v, a, d, n, metric))
+    orc = O.OracleIndex(v, a, d, n, int(metric))
+    # A radius around the 20th-nearest distance of the first query: both rounds run.
+    ids0, d0, _ = orc.search(q[:1], 40, 80, 1)
+    r = float(d0[0, 20])
+    inner = float(d0[0, 2])
+    for p in [Range(40, r), Range(40, r, inner_radius=inner), Range(40, r, beam_width=2),
+              Range(40, r, range_slack=1.3, initial_slack=0.5), Range(40, r, max_returned=60),
+              Range(8, r * 1.5, max_returned=120)]:
+        _assert_same(idx, orc, q, p, capacity=p.max_returned or 4000)
+
+
+def test_range_errors():
+    with pytest.raises(KnnSearchError):
+        Range(0, 1.0)
+    with pytest.raises(ANNError):
+        Range(10, 1.0, max_returned=5)
+    with pytest.raises(ANNError):
+        Range(10, 1.0, inner_radius=2.0)
+    v, a, d, n = random_index(500, 16, 8, seed=3, max_degree=8)
+    idx = DiskANNIndex(GpuProvider(v, a, d, n, Metric.L2))
+    with pytest.raises(ANNError) as e:
+        idx.range_search(Range(10, 1.0), v[:2, :8])
+    assert e.value.status == Status.DIMENSION_MISMATCH

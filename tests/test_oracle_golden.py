@@ -247,3 +247,24 @@ def test_oracle_pq_direct_cosine(dim, chunks):
         for j in range(10):
             want = _direct_cosine(q[i], pivots, offsets, codes[ids[i, j]])
             assert dists[i, j].view(np.uint32) == want.view(np.uint32)
+
+
+def _range_cases():
+    with open(os.path.join(GOLDEN, "range_search.json")) as f:
+        return json.load(f)
+
+
+@pytest.mark.parametrize("case", _range_cases(), ids=lambda c: c["source"].split("/")[-1][:-5])
+def test_oracle_matches_range_golden(case):
+    """Exact results, comparisons, hops and second-round flag of range_search.rs's baselines."""
+    v, a, d, n = datasets.grid(case["grid_dims"], case["grid_size"])
+    ix = O.OracleIndex(v, a, d, n, O.METRIC_L2)
+    ids, dists, st = ix.range_search(
+        np.array(case["query"], np.float32), case["starting_l"], case["radius"],
+        inner_radius=case["inner_radius"], initial_slack=case["initial_slack"],
+        range_slack=case["range_slack"], max_returned=case["max_returned"] or 0)
+    assert [[int(i), float(x)] for i, x in zip(ids, dists)] == case["results"]
+    assert int(st["cmps"]) == case["comparisons"]
+    assert int(st["hops"]) == case["hops"]
+    assert int(st["result_count"]) == case["result_count"]
+    assert bool(int(st["flags"]) & 2) == case["second_round"]
