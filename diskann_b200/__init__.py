@@ -19,6 +19,8 @@ from .index import (  # noqa: F401
     Metric,
     PQData,
     Quantized,
+    InmemProvider,
+    PagedSearch,
     Range,
     STATS_DTYPE,
     SearchServer,
@@ -27,5 +29,5 @@ from .index import (  # noqa: F401
 
 __all__ = [
     "ANNError", "BF16", "DiskANNIndex", "FP8", "FullPrecision", "GpuProvider", "Hybrid", "Knn",
-    "KnnSearchError", "Metric", "PQData", "Quantized", "Range", "STATS_DTYPE", "SearchServer", "Status",
+    "KnnSearchError", "Metric", "InmemProvider", "PQData", "PagedSearch", "Quantized", "Range", "STATS_DTYPE", "SearchServer", "Status",
 ]

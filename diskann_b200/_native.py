@@ -27,6 +27,12 @@ EXPORTED_SYMBOLS = (
     "dk_search_device_noalloc",
     "dk_range_search",
     "dk_range_search_device",
+    "dk_paged_search_create",
+    "dk_paged_search_next",
+    "dk_paged_search_destroy",
+    "dk_inmem_index_create",
+    "dk_inmem_set_tags",
+    "dk_inmem_search",
     "dk_server_create",
     "dk_server_submit",
     "dk_server_poll",
@@ -65,6 +71,23 @@ class IndexDesc(ctypes.Structure):
 
 INDEX_BF16 = 1
 INDEX_FP8 = 2
+
+
+class InmemDesc(ctypes.Structure):
+    _fields_ = [
+        ("capacity", ctypes.c_uint32),
+        ("num_frozen", ctypes.c_uint32),
+        ("dim", ctypes.c_uint32),
+        ("metric", ctypes.c_int32),
+        ("elem", ctypes.c_int32),
+        ("rows", ctypes.c_void_p),
+        ("row_stride", ctypes.c_uint64),
+        ("adjacency", ctypes.c_void_p),
+        ("adjacency_stride", ctypes.c_uint64),
+        ("degrees", ctypes.c_void_p),
+        ("max_degree", ctypes.c_uint32),
+        ("external_ids", ctypes.c_void_p),
+    ]
 
 
 class IndexInfo(ctypes.Structure):
@@ -143,6 +166,19 @@ def load():
         L.dk_range_search_device.restype = i32
         L.dk_range_search_device.argtypes = [vp, vp, u64, u32, u32, u32, f32, f32, f32, f32, u32,
                                              u32, vp, vp, vp, vp]
+        L.dk_paged_search_create.restype = i32
+        L.dk_paged_search_create.argtypes = [vp, vp, u64, u32, u32, vp, u32, u32,
+                                             ctypes.POINTER(vp)]
+        L.dk_paged_search_next.restype = i32
+        L.dk_paged_search_next.argtypes = [vp, u32, vp, vp, vp]
+        L.dk_paged_search_destroy.restype = i32
+        L.dk_paged_search_destroy.argtypes = [vp]
+        L.dk_inmem_index_create.restype = i32
+        L.dk_inmem_index_create.argtypes = [ctypes.POINTER(InmemDesc), i32, ctypes.POINTER(vp)]
+        L.dk_inmem_set_tags.restype = i32
+        L.dk_inmem_set_tags.argtypes = [vp, u32, u32, vp]
+        L.dk_inmem_search.restype = i32
+        L.dk_inmem_search.argtypes = [vp, vp, u64, u32, u32, u32, u32, vp, vp, vp]
         L.dk_search_device_noalloc.restype = i32
         L.dk_search_device_noalloc.argtypes = [vp, i32, vp, u64, u32, u32, u32, u32, vp, vp, vp, vp]
         L.dk_server_create.restype = i32

@@ -46,26 +46,15 @@ void free_index(dk_index* ix) {
   cudaFree(ix->vec_fp8);
   cudaFree(ix->bf16_meta);
   cudaFree(ix->fp8_meta);
+  cudaFree(ix->raw);
+  cudaFree(ix->readable);
+  cudaFree(ix->ext);
   cudaFree(ix->hint_dev);
   if (ix->hint_stage) cudaFreeHost(ix->hint_stage);
   if (ix->pool) cudaMemPoolDestroy(ix->pool);
   cudaSetDevice(prev);
   delete ix;
 }
-
-// Restores the caller's current device on scope exit.
-struct DeviceGuard {
-  int prev = -1;
-  explicit DeviceGuard(int dev) {
-    cudaGetDevice(&prev);
-    if (prev != dev) cudaSetDevice(dev);
-  }
-  ~DeviceGuard() {
-    int now = -1;
-    cudaGetDevice(&now);
-    if (prev >= 0 && now != prev) cudaSetDevice(prev);
-  }
-};
 
 
 }  // namespace
@@ -149,7 +138,7 @@ extern "C" int32_t dk_index_create(const dk_index_desc* d, int32_t device, dk_in
   cudaError_t e = cudaGetDeviceCount(&ndev);
   if (e != cudaSuccess) return cuda_fail(e, "cudaGetDeviceCount");
   if (device < 0 || device >= ndev) return fail(DK_ERR_INVALID_ARGUMENT, "no such CUDA device");
-  DeviceGuard guard(device);
+  dk::DeviceGuard guard(device);
 
   auto* ix = new dk_index();
   ix->device = device;
@@ -279,7 +268,7 @@ extern "C" int32_t dk_search_device(dk_index* ix, int32_t strategy, const float*
   if (v != DK_OK) return v;
   if (nq && (!queries || !ids || !dists || !stats))
     return fail(DK_ERR_INVALID_ARGUMENT, "queries, ids, dists and stats are required");
-  DeviceGuard guard(ix->device);
+  dk::DeviceGuard guard(ix->device);
   return dk_launch_search(ix, strategy, queries, query_stride, nq, k, l, beam_width, ids, dists,
                           stats, static_cast<cudaStream_t>(stream));
 }
@@ -292,7 +281,7 @@ extern "C" int32_t dk_search(dk_index* ix, int32_t strategy, const float* querie
   if (v != DK_OK) return v;
   if (nq == 0) return DK_OK;
   if (!queries || !ids || !dists) return fail(DK_ERR_INVALID_ARGUMENT, "queries, ids and dists are required");
-  DeviceGuard guard(ix->device);
+  dk::DeviceGuard guard(ix->device);
   cudaStream_t s = nullptr;
   cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
   if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");

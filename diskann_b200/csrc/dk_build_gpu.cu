@@ -45,19 +45,6 @@ int32_t cuda_fail(cudaError_t e, const char* what) {
   return fail(DK_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-struct DeviceGuard {
-  int prev = -1;
-  explicit DeviceGuard(int dev) {
-    cudaGetDevice(&prev);
-    if (prev != dev) cudaSetDevice(dev);
-  }
-  ~DeviceGuard() {
-    int now = -1;
-    cudaGetDevice(&now);
-    if (prev >= 0 && now != prev) cudaSetDevice(prev);
-  }
-};
-
 // Row r of `rows` (astride words: degree, ids, zero padding) goes to adjacency row nodes[r].
 __global__ void k_scatter_rows(uint32_t* __restrict__ adj, uint32_t astride,
                                const uint32_t* __restrict__ rows, const uint32_t* __restrict__ nodes,
@@ -98,7 +85,7 @@ int32_t dk_build_gpu_create(const float* vectors, uint64_t stride, uint32_t num_
     delete g;
     return rc;
   }
-  DeviceGuard guard(device);
+  dk::DeviceGuard guard(device);
   g->device = device;
   g->l_build = l_build;
   g->max_batch = max_batch;
@@ -126,7 +113,7 @@ int32_t dk_build_gpu_search(dk_build_gpu* g, uint32_t start, uint32_t count,
                             const uint32_t** rec_ids, const float** rec_d,
                             const uint32_t** hops, uint32_t* rec_cap) {
   if (count > g->max_batch) return fail(DK_ERR_INVALID_ARGUMENT, "build batch above max_batch");
-  DeviceGuard guard(g->device);
+  dk::DeviceGuard guard(g->device);
   dk_index* ix = g->ix;
   const SearchRecord rec{g->d_rec_ids, g->d_rec_d, g->rec_cap};
   int32_t rc = dk_launch_search(ix, DK_STRATEGY_FULL_PRECISION,
@@ -153,7 +140,7 @@ int32_t dk_build_gpu_search(dk_build_gpu* g, uint32_t start, uint32_t count,
 int32_t dk_build_gpu_set_rows(dk_build_gpu* g, const uint32_t* nodes, uint32_t count,
                               const std::vector<std::vector<uint32_t>>& adj) {
   if (count == 0) return DK_OK;
-  DeviceGuard guard(g->device);
+  dk::DeviceGuard guard(g->device);
   dk_index* ix = g->ix;
   const uint32_t astride = ix->astride;
   cudaError_t e = cudaSuccess;
@@ -199,7 +186,7 @@ int32_t dk_build_gpu_set_rows(dk_build_gpu* g, const uint32_t* nodes, uint32_t c
 void dk_build_gpu_destroy(dk_build_gpu* g) {
   if (!g) return;
   {
-    DeviceGuard guard(g->device);
+    dk::DeviceGuard guard(g->device);
     if (g->stream) cudaStreamSynchronize(g->stream);
     cudaFree(g->d_ids);
     cudaFree(g->d_dists);

@@ -47,6 +47,14 @@ struct dk_index {
   // freed memory reserved (release threshold: unlimited), so a repeated search reuses it
   // instead of mapping new memory each call.
   cudaMemPool_t pool = nullptr;
+  // diskann-inmem store (dk_inmem.cu): element type, rows of that type (raw_stride bytes,
+  // zero padded; FP32 indexes use `vectors`), readable-slot bits from the rows' tags, and the
+  // external id of each slot (DK_NO_EXTERNAL_ID: none).  Unset for other indexes.
+  int32_t elem = -1;
+  unsigned char* raw = nullptr;
+  uint32_t raw_stride = 0;
+  uint32_t* readable = nullptr;
+  uint64_t* ext = nullptr;
 };
 
 // Per-launch parameters of the beam-search kernels.
@@ -100,6 +108,11 @@ struct SearchParams {
   // Serving launches: per-request (k, L) pairs; outputs keep a stride of `k` (= max_k).
   // Null for batch launches, where every query uses `k` and `l`.
   const uint32_t* req_kl;
+  // diskann-inmem indexes: element rows of raw_stride bytes (FP16 / u8 / i8 modes), and the
+  // slots whose tag is readable (one bit per id); null elsewhere.
+  const unsigned char* raw;
+  uint32_t raw_stride;
+  const uint32_t* readable;
 };
 
 constexpr uint32_t kFlagSpilled = 1u;
@@ -109,6 +122,10 @@ constexpr int kModeFP32 = 0;
 constexpr int kModePQ = 1;
 constexpr int kModeBF16 = 2;
 constexpr int kModeFP8 = 3;
+// diskann-inmem element types (dk_inmem.cu): FP16 rows, and u8 / i8 rows scored in integers.
+constexpr int kModeF16 = 4;
+constexpr int kModeU8 = 5;
+constexpr int kModeI8 = 6;
 
 inline int mode_of_strategy(int32_t strategy) {
   switch (strategy) {
@@ -128,6 +145,22 @@ __host__ __device__ inline bool strategy_reranks(int32_t strategy) {
 
 // Thread-local error reporting for the C ABI.
 void dk_set_error(int32_t status, const std::string& msg);
+
+namespace dk {
+// Makes `dev` current for the scope and restores the caller's current device on exit.
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int now = -1;
+    cudaGetDevice(&now);
+    if (prev >= 0 && now != prev) cudaSetDevice(prev);
+  }
+};
+}  // namespace dk
 
 // Argument checks shared by every search entry point (sets the thread's error).
 int32_t dk_check_search_args(const dk_index* ix, int32_t strategy, uint32_t k, uint32_t l,

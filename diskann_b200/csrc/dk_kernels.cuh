@@ -301,11 +301,28 @@ __device__ __forceinline__ void acc4(float4 a, float4 v, float* acc) {
   }
 }
 
+// Row elements as floats: FP32 rows directly, FP16 rows (the diskann-inmem f16 layer) through
+// the exact f16 -> f32 conversion.  ld4 reads elements 4i..4i+3, ld1 element i.
+__device__ __forceinline__ float4 ld4(const float* r, uint32_t i) {
+  return __ldg(reinterpret_cast<const float4*>(r) + i);
+}
+__device__ __forceinline__ float4 ld4(const __half* r, uint32_t i) {
+  const uint2 w = __ldg(reinterpret_cast<const uint2*>(r) + i);
+  const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&w.x));
+  const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&w.y));
+  return make_float4(a.x, a.y, b.x, b.y);
+}
+__device__ __forceinline__ float ld1(const float* r, uint32_t i) { return __ldg(r + i); }
+__device__ __forceinline__ float ld1(const __half* r, uint32_t i) { return __half2float(r[i]); }
+
 // Distances of U rows to the shared-memory query `q` (zero padded to a multiple of 8
-// floats) computed by the 8 lanes of a subgroup; rows are padded to 4 floats and 16-byte
-// aligned.  All 8 lanes return the results.  L2, inner product, normalised cosine.
-template <int METRIC, int DIM, int U>
-__device__ __forceinline__ void subgroup_distances(const float* const (&rows)[U],
+// floats) computed by the 8 lanes of a subgroup; rows are padded to 4 elements and aligned to
+// 4 elements.  All 8 lanes return the results.  L2, inner product, normalised cosine.  FP16
+// rows take the same path: the reference's f32-by-f16 kernels (simd.rs:1121-1156, 1878-1912,
+// Strategy4x2) feed the same vectors to the same accumulators in the same order as
+// Strategy4x1, after an exact conversion.
+template <int METRIC, int DIM, int U, class RowT = float>
+__device__ __forceinline__ void subgroup_distances(const RowT* const (&rows)[U],
                                                    const float* __restrict__ q, uint32_t dim_rt,
                                                    uint32_t s, unsigned gmask, float (&out)[U]) {
   const uint32_t dim = DIM > 0 ? (uint32_t)DIM : dim_rt;
@@ -324,7 +341,7 @@ __device__ __forceinline__ void subgroup_distances(const float* const (&rows)[U]
     for (int u = 0; u < U; ++u)
 #pragma unroll
       for (int b = 0; b < NB; ++b)
-        v[u][b] = __ldg(reinterpret_cast<const float4*>(rows[u]) + 8 * b + s);
+        v[u][b] = ld4(rows[u], 8 * b + s);
 #pragma unroll
     for (int b = 0; b < NB; ++b) {
       const float4 a = q4[8 * b + s];
@@ -337,7 +354,7 @@ __device__ __forceinline__ void subgroup_distances(const float* const (&rows)[U]
       const float4 a = q4[base >> 2];
       float4 v[U];
 #pragma unroll
-      for (int u = 0; u < U; ++u) v[u] = __ldg(reinterpret_cast<const float4*>(rows[u]) + (base >> 2));
+      for (int u = 0; u < U; ++u) v[u] = ld4(rows[u], base >> 2);
 #pragma unroll
       for (int u = 0; u < U; ++u) acc4<METRIC>(a, v[u], acc[u]);
     }
@@ -356,7 +373,7 @@ __device__ __forceinline__ void subgroup_distances(const float* const (&rows)[U]
       const float av[4] = {a.x, a.y, a.z, a.w};
 #pragma unroll
       for (int u = 0; u < U; ++u) {
-        const float4 v = __ldg(reinterpret_cast<const float4*>(rows[u]) + (e >> 2));
+        const float4 v = ld4(rows[u], e >> 2);
         const float vv[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
@@ -388,8 +405,8 @@ __device__ __forceinline__ void subgroup_distances(const float* const (&rows)[U]
 // element 8k + s.  sum (simd.rs:2327-2361): sum_tree of each accumulator (xor 4, 2, 1 over the
 // 8 lanes gives (t_i + t_{i+4}), then (q0 + q2) + (q1 + q3)); zero similarity if a norm is
 // below f32::MIN_POSITIVE, else clamp(prod / (sqrt(nx) * sqrt(ny))); distance 1 - similarity.
-template <int DIM>
-__device__ __forceinline__ float subgroup_cosine(const float* __restrict__ row,
+template <int DIM, class RowT = float>
+__device__ __forceinline__ float subgroup_cosine(const RowT* __restrict__ row,
                                                  const float* __restrict__ q, uint32_t dim_rt,
                                                  uint32_t s, unsigned gmask) {
   const uint32_t dim = DIM > 0 ? (uint32_t)DIM : dim_rt;
@@ -398,7 +415,7 @@ __device__ __forceinline__ float subgroup_cosine(const float* __restrict__ row,
   uint32_t k = 0;
 #pragma unroll 8
   for (; k + 1u < nvec; k += 2u) {
-    const float b0 = __ldg(row + 8u * k + s), b1 = __ldg(row + 8u * k + 8u + s);
+    const float b0 = ld1(row, 8u * k + s), b1 = ld1(row, 8u * k + 8u + s);
     const float a0 = q[8u * k + s], a1 = q[8u * k + 8u + s];
     x0 = __fmaf_rn(a0, a0, x0);
     y0 = __fmaf_rn(b0, b0, y0);
@@ -408,14 +425,14 @@ __device__ __forceinline__ float subgroup_cosine(const float* __restrict__ row,
     p1 = __fmaf_rn(a1, b1, p1);
   }
   if (k < nvec) {
-    const float b0 = __ldg(row + 8u * k + s), a0 = q[8u * k + s];
+    const float b0 = ld1(row, 8u * k + s), a0 = q[8u * k + s];
     x0 = __fmaf_rn(a0, a0, x0);
     y0 = __fmaf_rn(b0, b0, y0);
     p0 = __fmaf_rn(a0, b0, p0);
   }
   float tx = x0 + x1, ty = y0 + y1, tp = p0 + p1;
   if (s < (dim & 7u)) {
-    const float b = __ldg(row + 8u * nvec + s), a = q[8u * nvec + s];
+    const float b = ld1(row, 8u * nvec + s), a = q[8u * nvec + s];
     tx = __fmaf_rn(a, a, tx);
     ty = __fmaf_rn(b, b, ty);
     tp = __fmaf_rn(a, b, tp);
@@ -435,26 +452,37 @@ __device__ __forceinline__ float subgroup_cosine(const float* __restrict__ row,
 
 // Score candidates ids[0..count) into d[...] with subgroup `sg` of `nsub` subgroups; U rows
 // per subgroup are loaded together.  Lanes of a subgroup must be converged.
-template <int METRIC, int DIM, int U>
+template <class RowT>
+__device__ __forceinline__ const RowT* row_of(const SearchParams& P, uint32_t id);
+template <>
+__device__ __forceinline__ const float* row_of<float>(const SearchParams& P, uint32_t id) {
+  return P.vectors + (size_t)id * P.vstride;
+}
+template <>
+__device__ __forceinline__ const __half* row_of<__half>(const SearchParams& P, uint32_t id) {
+  return reinterpret_cast<const __half*>(P.raw + (size_t)id * P.raw_stride);
+}
+
+template <int METRIC, int DIM, int U, class RowT = float>
 __device__ __forceinline__ void score_fp(const SearchParams& P, const float* q,
                                          const uint32_t* ids, float* d, uint32_t count,
                                          uint32_t sg, uint32_t nsub, uint32_t s, unsigned gmask) {
   if (METRIC == DK_METRIC_COSINE) {
     for (uint32_t i = sg; i < count; i += nsub) {
-      const float r = subgroup_cosine<DIM>(P.vectors + (size_t)ids[i] * P.vstride, q, P.dim, s, gmask);
+      const float r = subgroup_cosine<DIM>(row_of<RowT>(P, ids[i]), q, P.dim, s, gmask);
       if (s == 0) d[i] = r;
     }
     return;
   }
   const uint32_t step = nsub * U;
   for (uint32_t base = 0; base < count; base += step) {
-    const float* rows[U];
+    const RowT* rows[U];
     uint32_t idx[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       idx[u] = base + sg + u * nsub;
       const uint32_t j = idx[u] < count ? idx[u] : count - 1;  // a valid row; result unused
-      rows[u] = P.vectors + (size_t)ids[j] * P.vstride;
+      rows[u] = row_of<RowT>(P, ids[j]);
     }
     float out[U];
     subgroup_distances<METRIC, DIM, U>(rows, q, P.dim, s, gmask, out);
@@ -463,6 +491,76 @@ __device__ __forceinline__ void score_fp(const SearchParams& P, const float* q,
       for (int u = 0; u < U; ++u)
         if (idx[u] < count) d[idx[u]] = out[u];
     }
+  }
+}
+
+// Integer rows (the diskann-inmem u8 / i8 layers): the reference accumulates x*x, y*y, x*y or
+// (x-y)^2 exactly in i32 lanes (simd.rs:1192-1227, 1370-1405, 1947-1981, 2109-2145,
+// 2790-2829, 2996-3035) and converts the sums to f32 once, so the order of the additions does
+// not matter.  Lane s of a subgroup takes 4-byte words s, s+8, ... of the row and the packed
+// query (both zero padded) with dp4a; L2 = xx + yy - 2xy in 64-bit, exact.  The f32 post-ops
+// are the reference's: L2 the sum, inner product its negation, cosine 1 - clamp(xy / (sqrt(xx)
+// sqrt(yy))) with zero similarity below f32::MIN_POSITIVE (simd.rs:2327-2363).  Exact while
+// no i32 sum of the reference wraps (dim <= 33,000 for u8).
+template <int METRIC, bool SIGNED>
+__device__ __forceinline__ void score_int(const SearchParams& P, const float* q,
+                                          const uint32_t* ids, float* d, uint32_t count,
+                                          uint32_t sg, uint32_t nsub, uint32_t s, unsigned gmask) {
+  const uint32_t* qw = reinterpret_cast<const uint32_t*>(q);
+  const uint32_t nw = (P.dim + 3u) >> 2;
+  for (uint32_t i = sg; i < count; i += nsub) {
+    const uint32_t* row = reinterpret_cast<const uint32_t*>(P.raw + (size_t)ids[i] * P.raw_stride);
+    long long xx, yy, xy;
+    if (SIGNED) {
+      int a2 = 0, b2 = 0, ab = 0;
+      for (uint32_t w = s; w < nw; w += 8u) {
+        const int a = (int)qw[w], b = (int)__ldg(row + w);
+        a2 = __dp4a(a, a, a2);
+        b2 = __dp4a(b, b, b2);
+        ab = __dp4a(a, b, ab);
+      }
+#pragma unroll
+      for (int o = 4; o > 0; o >>= 1) {
+        a2 += __shfl_xor_sync(gmask, a2, o, 8);
+        b2 += __shfl_xor_sync(gmask, b2, o, 8);
+        ab += __shfl_xor_sync(gmask, ab, o, 8);
+      }
+      xx = a2;
+      yy = b2;
+      xy = ab;
+    } else {
+      unsigned a2 = 0u, b2 = 0u, ab = 0u;
+      for (uint32_t w = s; w < nw; w += 8u) {
+        const unsigned a = qw[w], b = __ldg(row + w);
+        a2 = __dp4a(a, a, a2);
+        b2 = __dp4a(b, b, b2);
+        ab = __dp4a(a, b, ab);
+      }
+#pragma unroll
+      for (int o = 4; o > 0; o >>= 1) {
+        a2 += __shfl_xor_sync(gmask, a2, o, 8);
+        b2 += __shfl_xor_sync(gmask, b2, o, 8);
+        ab += __shfl_xor_sync(gmask, ab, o, 8);
+      }
+      xx = a2;
+      yy = b2;
+      xy = ab;
+    }
+    if (s != 0) continue;
+    float r;
+    if (METRIC == DK_METRIC_L2) {
+      r = __ll2float_rn(xx + yy - 2 * xy);
+    } else if (METRIC == DK_METRIC_INNER_PRODUCT) {
+      r = -__ll2float_rn(xy);
+    } else {  // cosine; the layers map CosineNormalized to cosine for integer data
+      const float nx = __ll2float_rn(xx), ny = __ll2float_rn(yy), p = __ll2float_rn(xy);
+      const float denom = __fmul_rn(__fsqrt_rn(nx), __fsqrt_rn(ny));
+      float sim;
+      if (nx < 1.17549435e-38f || ny < 1.17549435e-38f) sim = 0.0f;
+      else sim = fmaxf(-1.0f, fminf(1.0f, __fdiv_rn(p, denom)));
+      r = 1.0f - sim;
+    }
+    d[i] = r;
   }
 }
 
@@ -907,6 +1005,10 @@ __device__ __forceinline__ void cta_score(const SearchParams& P, const State& S,
     const unsigned gmask = 0xFFu << (8u * ((tid & 31u) >> 3));
     if constexpr (MODE == kModeFP32) {
       score_fp<METRIC, DIM, 1>(P, S.q, ids, d, count, tid >> 3, NT / 8, tid & 7u, gmask);
+    } else if constexpr (MODE == kModeF16) {
+      score_fp<METRIC, DIM, 1, __half>(P, S.q, ids, d, count, tid >> 3, NT / 8, tid & 7u, gmask);
+    } else if constexpr (MODE == kModeU8 || MODE == kModeI8) {
+      score_int<METRIC, MODE == kModeI8>(P, S.q, ids, d, count, tid >> 3, NT / 8, tid & 7u, gmask);
     } else if constexpr (DIM > 0) {
       score_lp_wide<METRIC, MODE, DIM>(P, S.q, ids, d, count, tid >> 3, NT / 8, tid & 7u, gmask);
     } else {
@@ -1089,6 +1191,10 @@ __device__ bool cta_search(const SearchParams& P, const State& S, const VSet& vs
         if (t < deg) {
           id = __ldg(row + 1 + t);
           fresh = vset.insert(id);
+          // diskann-inmem (provider.rs:451-473): a slot whose tag is not readable stays in the
+          // visited set but is not scored.  Only set with the exact bitmap visited set, so
+          // `inserted` (hash load) needs no count of these.
+          if (fresh && P.readable) fresh = (__ldg(P.readable + (id >> 5)) >> (id & 31u)) & 1u;
         }
         uint32_t total;
         const uint32_t pos = block_scan<NT>(fresh, M->warp_sums, total);
@@ -1584,10 +1690,13 @@ __device__ __forceinline__ void warp_query(const SearchParams& P, const State& S
 // Persistent grid: every warp owns a shared-memory slice and a global overflow table and
 // takes queries from a work counter until the batch is done.
 template <int METRIC, int MODE, int DIM, int U>
-// The explicit minimum of one resident block lets the compiler give each thread up to 255
-// registers; it takes ~170 here, and the kernel measured ~1.6x faster that way than with the
-// compiler's own choice for `__launch_bounds__(128)` alone (96 registers and spills).
-__global__ void __launch_bounds__(128, 1) k_search_warp(const SearchParams P) {
+// FP32 / PQ: the explicit minimum of one resident block lets the compiler give each thread up
+// to 255 registers; it takes ~170 here, and the kernel measured ~1.6x faster that way than with
+// the compiler's own choice for `__launch_bounds__(128)` alone (96 registers and spills).
+// BF16 / FP8: a minimum of four blocks caps them at 128 registers (121-127 used, no spills),
+// measured 5-9% faster on a 1M-point graph than with ~160 registers.
+__global__ void __launch_bounds__(128, (MODE == kModeBF16 || MODE == kModeFP8) ? 4 : 1)
+    k_search_warp(const SearchParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
   const uint32_t slot = blockIdx.x * (blockDim.x >> 5) + warp;

@@ -182,19 +182,6 @@ int32_t fail(int32_t status, const std::string& msg) {
   return status;
 }
 
-struct DeviceGuard {
-  int prev = -1;
-  explicit DeviceGuard(int dev) {
-    cudaGetDevice(&prev);
-    if (prev != dev) cudaSetDevice(dev);
-  }
-  ~DeviceGuard() {
-    int now = -1;
-    cudaGetDevice(&now);
-    if (prev >= 0 && now != prev) cudaSetDevice(prev);
-  }
-};
-
 // Range::with_options validation (range_search.rs:63-110) plus this API's own bounds.
 int32_t check_range(const dk_index* ix, uint32_t starting_l, uint32_t beam_width, float radius,
                     float inner_radius, float initial_slack, float range_slack,
@@ -273,7 +260,7 @@ extern "C" int32_t dk_range_search_device(dk_index* ix, const float* queries,
   if (v != DK_OK) return v;
   if (nq && (!queries || !ids || !dists || !stats))
     return fail(DK_ERR_INVALID_ARGUMENT, "queries, ids, dists and stats are required");
-  DeviceGuard guard(ix->device);
+  dk::DeviceGuard guard(ix->device);
   const RangeParams R{radius, inner_radius, initial_slack, range_slack, starting_l, max_returned,
                       capacity};
   return launch_range_search(ix, queries, query_stride, nq, R, beam_width, ids, dists, stats,
@@ -290,7 +277,7 @@ extern "C" int32_t dk_range_search(dk_index* ix, const float* queries, uint64_t 
   if (v != DK_OK) return v;
   if (nq == 0) return DK_OK;
   if (!queries || !ids || !dists) return fail(DK_ERR_INVALID_ARGUMENT, "queries, ids and dists are required");
-  DeviceGuard guard(ix->device);
+  dk::DeviceGuard guard(ix->device);
   cudaStream_t s = nullptr;
   cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
   if (e != cudaSuccess) return fail(DK_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));

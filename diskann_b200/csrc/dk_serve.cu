@@ -84,19 +84,6 @@ int32_t cuda_fail(cudaError_t e, const char* what) {
   return fail(DK_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-struct DeviceGuard {
-  int prev = -1;
-  explicit DeviceGuard(int dev) {
-    cudaGetDevice(&prev);
-    if (prev != dev) cudaSetDevice(dev);
-  }
-  ~DeviceGuard() {
-    int now = -1;
-    cudaGetDevice(&now);
-    if (prev >= 0 && now != prev) cudaSetDevice(prev);
-  }
-};
-
 void release(dk_server* s) {
   for (Context& c : s->ctx) {
     if (c.stream) cudaStreamSynchronize(c.stream);
@@ -211,7 +198,7 @@ extern "C" int32_t dk_server_create(dk_index* ix, const dk_server_config* cfg, d
   if (cfg->beam_width > 4)
     return fail(DK_ERR_UNSUPPORTED, "serving runs beam_width <= 4 (one warp per request)");
   if (cfg->streams > 64) return fail(DK_ERR_INVALID_ARGUMENT, "streams above 64");
-  DeviceGuard guard(ix->device);
+  dk::DeviceGuard guard(ix->device);
   dk_server* s = new dk_server();
   s->ix = ix;
   s->cfg = *cfg;
@@ -305,7 +292,7 @@ extern "C" int32_t dk_server_submit(dk_server* s, const float* query, uint32_t k
   s->state[r] = kPending;
   s->pending.push_back(t);
   *ticket = t;
-  DeviceGuard guard(s->ix->device);
+  dk::DeviceGuard guard(s->ix->device);
   return progress(s);
 }
 
@@ -317,7 +304,7 @@ extern "C" int32_t dk_server_poll(dk_server* s, uint64_t ticket, uint32_t* ids, 
   const uint32_t r = (uint32_t)(ticket % depth);
   if (ticket >= s->next_ticket || ticket < s->head || s->state[r] == kFree)
     return fail(DK_ERR_NOT_FOUND, "unknown or already collected ticket");
-  DeviceGuard guard(s->ix->device);
+  dk::DeviceGuard guard(s->ix->device);
   if (s->state[r] != kDone) {
     const int32_t rc = progress(s);
     if (rc != DK_OK) return rc;
@@ -380,7 +367,7 @@ extern "C" int32_t dk_server_replay(dk_server* s, const float* queries, uint64_t
                std::chrono::steady_clock::now() - t0).count();
   };
   uint32_t next = 0, done = 0;
-  DeviceGuard guard(s->ix->device);
+  dk::DeviceGuard guard(s->ix->device);
   while (done < n) {
     std::lock_guard<std::mutex> lock(s->mu);
     // Submit every request whose arrival time has come, while admission allows.
@@ -458,7 +445,7 @@ extern "C" int32_t dk_server_get_info(const dk_server* s, dk_server_info* info) 
 
 extern "C" int32_t dk_server_destroy(dk_server* s) {
   if (!s) return DK_OK;
-  DeviceGuard guard(s->ix->device);
+  dk::DeviceGuard guard(s->ix->device);
   release(s);  // waits for launches in flight; uncollected results are dropped
   return DK_OK;
 }

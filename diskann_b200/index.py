@@ -254,6 +254,99 @@ class GpuProvider:
             pass
 
 
+# diskann-inmem store (diskann-inmem/src/store.rs, tag.rs): element types and tags.
+ELEM_TYPES = {"f32": (0, np.float32), "f16": (1, np.float16), "u8": (2, np.uint8),
+              "i8": (3, np.int8)}
+TAG_AVAILABLE, TAG_OWNED, TAG_RETIRING, TAG_PUBLISHED, TAG_FROZEN = 0, 1, 2, 254, 255
+NO_EXTERNAL_ID = 0xFFFFFFFFFFFFFFFF
+
+
+def inmem_rows(vectors, tags) -> np.ndarray:
+    """Store slots as the diskann-inmem store lays them out (store.rs:150-260): each row's
+    element bytes, then its one-byte tag, padded to a multiple of 32 bytes."""
+    v = np.ascontiguousarray(vectors)
+    raw = v.view(np.uint8).reshape(v.shape[0], -1)
+    stride = -(-(raw.shape[1] + 1) // 32) * 32
+    rows = np.zeros((v.shape[0], stride), dtype=np.uint8)
+    rows[:, : raw.shape[1]] = raw
+    rows[:, raw.shape[1]] = np.asarray(tags, dtype=np.uint8)
+    return rows
+
+
+class InmemProvider:
+    """The diskann-inmem provider's store on the GPU (``dk_inmem_index_create``).
+
+    ``vectors``: (capacity + F, D) of the element type (float32 / float16 / uint8 / int8),
+    the last F rows the frozen start points; ``tags``: per slot (``TAG_PUBLISHED`` /
+    ``TAG_FROZEN`` readable, anything else not); ``external_ids``: per slot (uint64,
+    ``NO_EXTERNAL_ID`` = none).  ``search`` runs the provider's search with its Translate
+    post-processor and returns external ids.
+    """
+
+    def __init__(self, vectors, adjacency, degrees, capacity: int, tags, external_ids,
+                 metric=Metric.L2, device: int = 0):
+        v = np.ascontiguousarray(vectors)
+        elem = next((code for code, dt in ELEM_TYPES.values() if v.dtype == dt), None)
+        if elem is None:
+            raise ANNError(Status.INVALID_ARGUMENT, f"unsupported element type {v.dtype}")
+        rows = inmem_rows(v, tags)
+        adjacency = np.ascontiguousarray(adjacency, dtype=np.uint32)
+        degrees = np.ascontiguousarray(degrees, dtype=np.uint32)
+        ext = np.ascontiguousarray(external_ids, dtype=np.uint64)
+        d = _native.InmemDesc()
+        d.capacity = int(capacity)
+        d.num_frozen = v.shape[0] - int(capacity)
+        d.dim = v.shape[1]
+        d.metric = int(metric)
+        d.elem = elem
+        d.rows = rows.ctypes.data
+        d.row_stride = rows.shape[1]
+        d.adjacency = adjacency.ctypes.data
+        d.adjacency_stride = adjacency.shape[1]
+        d.degrees = degrees.ctypes.data
+        d.max_degree = adjacency.shape[1]
+        d.external_ids = ext.ctypes.data
+        handle = ctypes.c_void_p()
+        _check(_native.load().dk_inmem_index_create(ctypes.byref(d), int(device),
+                                                    ctypes.byref(handle)))
+        self._handle = handle
+        self.dtype = v.dtype
+        self.dim = v.shape[1]
+        self.capacity = int(capacity)
+        self.metric = Metric(int(metric))
+
+    def set_tags(self, first: int, tags) -> None:
+        t = np.ascontiguousarray(tags, dtype=np.uint8)
+        _check(_native.load().dk_inmem_set_tags(self._handle, int(first), t.size, t.ctypes.data))
+
+    def search(self, params: "Knn", queries):
+        """Search a batch of queries of the element type; returns ``(ids, dists, stats)`` with
+        external ids (uint64, ``NO_EXTERNAL_ID`` where fewer than k results)."""
+        q = np.ascontiguousarray(np.atleast_2d(queries), dtype=self.dtype)
+        if q.shape[1] != self.dim:
+            raise ANNError(Status.DIMENSION_MISMATCH, f"query dim {q.shape[1]} != {self.dim}")
+        nq, k = q.shape[0], params.k_value
+        ids = np.empty((nq, k), dtype=np.uint64)
+        dists = np.empty((nq, k), dtype=np.float32)
+        stats = np.zeros(nq, dtype=STATS_DTYPE)
+        _check(_native.load().dk_inmem_search(self._handle, q.ctypes.data, q.shape[1], nq, k,
+                                              params.l_value, params.beam_width,
+                                              ids.ctypes.data, dists.ctypes.data,
+                                              stats.ctypes.data))
+        return ids, dists, stats
+
+    def close(self) -> None:
+        if getattr(self, "_handle", None) is not None:
+            _native.load().dk_index_destroy(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class DiskANNIndex:
     """Graph index over a :class:`GpuProvider`; ``search`` runs batched greedy beam search."""
 
@@ -302,6 +395,12 @@ class DiskANNIndex:
                for i in range(nq)]
         return out, stats
 
+    def paged_search(self, queries, l_value: int, init_ids=None, queue_capacity: int = 0):
+        """Start a paged search for each query (FullPrecision, ``dk_paged_search_create``;
+        index.rs:2080-2160 ``paged_search`` / ``paged_search_with_init_ids``).  ``init_ids``:
+        None for the start points, or ``(nq, n_init)`` ids.  Returns a :class:`PagedSearch`."""
+        return PagedSearch(self, queries, l_value, init_ids, queue_capacity)
+
     def search_device(self, params: Knn, strategy: _Strategy, queries, ids, dists, stats,
                       stream=None) -> None:
         """Search device-resident queries; outputs go to caller-allocated device buffers.
@@ -321,6 +420,55 @@ class DiskANNIndex:
             params.k_value, params.l_value, params.beam_width, ids.data_ptr(), dists.data_ptr(),
             stats.data_ptr(), ctypes.c_void_p(handle),
         ))
+
+
+class PagedSearch:
+    """Paged-search sessions, one per query (``dk_paged_search_*``; paged.rs).
+
+    ``next_page(k)`` returns ``(pages, stats)``: per query the ``(ids, dists)`` of its next
+    page of at most ``k`` results (empty once its search is exhausted), and the stats array
+    (running ``cmps`` / ``hops``; flags bit 2: the session's queue filled).  Raises
+    ``ANNError`` (``INVALID_ARGUMENT``) for ``k == 0`` or ``k > l_value`` like the reference.
+    """
+
+    def __init__(self, index: "DiskANNIndex", queries, l_value: int, init_ids=None,
+                 queue_capacity: int = 0):
+        q = np.ascontiguousarray(np.atleast_2d(queries), dtype=np.float32)
+        prov = index.provider
+        if q.shape[1] != prov.dim:
+            raise ANNError(Status.DIMENSION_MISMATCH, f"query dim {q.shape[1]} != {prov.dim}")
+        init = None
+        if init_ids is not None:
+            init = np.ascontiguousarray(np.atleast_2d(init_ids), dtype=np.uint32)
+            if init.shape[0] != q.shape[0]:
+                raise ANNError(Status.INVALID_ARGUMENT, "init_ids needs one row per query")
+        self._index = index
+        self.nq = q.shape[0]
+        self.l_value = int(l_value)
+        handle = ctypes.c_void_p()
+        _check(_native.load().dk_paged_search_create(
+            prov.handle, q.ctypes.data, q.shape[1], self.nq, self.l_value,
+            None if init is None else init.ctypes.data, 0 if init is None else init.shape[1],
+            queue_capacity, ctypes.byref(handle)))
+        self._h = handle
+
+    def next_page(self, k: int):
+        ids = np.empty((self.nq, max(k, 1)), dtype=np.uint32)
+        dists = np.empty((self.nq, max(k, 1)), dtype=np.float32)
+        stats = np.zeros(self.nq, dtype=STATS_DTYPE)
+        _check(_native.load().dk_paged_search_next(self._h, k, ids.ctypes.data,
+                                                   dists.ctypes.data, stats.ctypes.data))
+        pages = [(ids[i, : stats[i]["result_count"]], dists[i, : stats[i]["result_count"]])
+                 for i in range(self.nq)]
+        return pages, stats
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            _native.load().dk_paged_search_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
 
 
 class SearchServer:

@@ -184,6 +184,69 @@ int32_t dk_range_search_device(dk_index* index, const float* queries, uint64_t q
                                float range_slack, uint32_t max_returned, uint32_t capacity,
                                uint32_t* ids, float* dists, dk_search_stats* stats, void* stream);
 
+/* Paged search with the FullPrecision strategy, one session per query of a batch.
+ * dk_paged_search_create replaces DiskANNIndex::paged_search / paged_search_with_init_ids
+ * (diskann/src/graph/index.rs:2080-2160): the init ids (init_ids = NULL / n_init = 0: the start
+ * points; else n_init ids per query, row-major) enter the visited set and their neighbours
+ * seed a queue that keeps every scored id (the reference's resizable queue; search window
+ * l_value + F).  dk_paged_search_next replaces PagedSearch::next_page
+ * (diskann/src/graph/search/paged.rs:52-151) for every session at once: up to k results per
+ * session (ids / dists: nq x k host arrays; result_count in stats says how many, 0 once the
+ * session is exhausted), resuming the search where the previous page stopped; pages never
+ * repeat an id.  Errors: k == 0 or k > l_value -> DK_ERR_INVALID_ARGUMENT (the reference's
+ * paged-search error).  stats carry each session's running comparison and hop counts.  The
+ * queue holds queue_capacity entries per session (0 = N + F, which can never fill); a session
+ * whose queue filled keeps its best entries and reports flags bit 2.  Device memory per
+ * session: 8 * queue_capacity + (N + F) / 8 + 16 * l_value bytes, plus the query. */
+typedef struct dk_paged dk_paged;
+int32_t dk_paged_search_create(dk_index* index, const float* queries, uint64_t query_stride,
+                               uint32_t nq, uint32_t l_value, const uint32_t* init_ids,
+                               uint32_t n_init, uint32_t queue_capacity, dk_paged** out);
+int32_t dk_paged_search_next(dk_paged* search, uint32_t k, uint32_t* ids, float* dists,
+                             dk_search_stats* stats);
+int32_t dk_paged_search_destroy(dk_paged* search);
+
+/* The diskann-inmem provider (diskann-inmem/src/provider.rs), its store and search.
+ *
+ * dk_inmem_index_create replaces diskann_inmem::Provider::new plus the inserts that filled it:
+ * it takes the provider's store as it lies in memory - one slot of `row_stride` bytes per id,
+ * `dim` elements of `elem` followed by the one-byte concurrency tag (store.rs:150-260; the
+ * frozen start points are the last `num_frozen` slots, store.rs:248-251) - its adjacency
+ * lists and, per slot, the external id (ids.rs IdMap; DK_NO_EXTERNAL_ID: no mapping, as for
+ * the frozen slots and deleted or empty ones).  A slot is readable when its tag is PUBLISHED
+ * (254) or FROZEN (255) (tag.rs Tag::can_read); every frozen slot must be.
+ *
+ * dk_inmem_search replaces DiskANNIndex::search with the provider's Strategy and default
+ * post-processor (provider.rs:855-960): the search loop of dk_search where a neighbour whose
+ * slot is not readable enters the visited set but is not scored (provider.rs:451-473), and
+ * results are the queue's entries that have an external id, in order, translated (Translate,
+ * provider.rs:906-945); `ids` receives the external ids.  Queries are `elem` values
+ * (query_stride in elements); f16 data is searched with f32 queries converted from f16, as
+ * the f16 layer does (layers/full.rs:404-437).  u8 / i8 with CosineNormalized use cosine, as
+ * the layers do.  Host buffers; returns when the results are written.
+ * dk_inmem_set_tags updates the tags of slots [first, first + count) (deletes, inserts). */
+enum dk_elem { DK_ELEM_F32 = 0, DK_ELEM_F16 = 1, DK_ELEM_U8 = 2, DK_ELEM_I8 = 3 };
+#define DK_NO_EXTERNAL_ID 0xFFFFFFFFFFFFFFFFull
+typedef struct dk_inmem_desc {
+  uint32_t capacity;          /* data slots 0..capacity-1 (the provider's Config::capacity) */
+  uint32_t num_frozen;        /* start points: slots capacity..capacity+num_frozen-1 */
+  uint32_t dim;
+  int32_t metric;             /* enum dk_metric */
+  int32_t elem;               /* enum dk_elem */
+  const uint8_t* rows;        /* (capacity + num_frozen) slots of row_stride bytes */
+  uint64_t row_stride;        /* >= dim * element size + 1 */
+  const uint32_t* adjacency;  /* (capacity + num_frozen) rows of adjacency_stride ids */
+  uint64_t adjacency_stride;
+  const uint32_t* degrees;
+  uint32_t max_degree;
+  const uint64_t* external_ids; /* per slot */
+} dk_inmem_desc;
+int32_t dk_inmem_index_create(const dk_inmem_desc* desc, int32_t device, dk_index** out);
+int32_t dk_inmem_set_tags(dk_index* index, uint32_t first, uint32_t count, const uint8_t* tags);
+int32_t dk_inmem_search(dk_index* index, const void* queries, uint64_t query_stride, uint32_t nq,
+                        uint32_t k, uint32_t l, uint32_t beam_width, uint64_t* ids, float* dists,
+                        dk_search_stats* stats);
+
 /* Same search, arguments and results as dk_search_device, for callers that cannot allocate
  * device memory while they search: for example a process whose own caching allocator took the
  * GPU's free memory at start-up (so the allocation inside dk_search_device would fail), or a

@@ -19,6 +19,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cfloat>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -186,6 +187,7 @@ struct Queue {
   size_t capacity = 0;
   size_t cursor = 0;
   size_t search_l = 0;
+  bool resizable = false;  // queue.rs:108-119 auto_resizable: never drops, grows instead
 
   explicit Queue(size_t cap) : capacity(cap), search_l(cap) {
     ids.reserve(cap + 1);
@@ -203,7 +205,11 @@ struct Queue {
   // queue.rs:130-171 `insert`.
   void insert(uint32_t id, float d) {
     if (std::isnan(d)) return;
-    if (size == capacity && dists[size - 1] < d) return;
+    if (resizable) {
+      if (size == capacity) capacity += std::max<size_t>(1, capacity >> 1);  // 1.5x
+    } else if (size == capacity && dists[size - 1] < d) {
+      return;
+    }
     const size_t idx = size > 0 ? lower_bound(d) : 0;
     if (size == capacity) {
       ids.pop_back();
@@ -234,6 +240,16 @@ struct Queue {
 
   // queue.rs:190-193 `iter`: first min(search_l, size) entries.
   size_t iter_len() const { return std::min(search_l, size); }
+
+  // queue.rs:174-181 `drain_best`: drop the first `count` entries; the cursor restarts at 0.
+  void drain_best(size_t count) {
+    count = std::min(count, size);
+    ids.erase(ids.begin(), ids.begin() + count);
+    visited.erase(visited.begin(), visited.begin() + count);
+    dists.erase(dists.begin(), dists.begin() + count);
+    size -= count;
+    cursor = 0;
+  }
 };
 
 // Visited set: an open-addressing u32 set with linear probing that doubles at 50% load.
@@ -487,6 +503,98 @@ extern "C" int32_t orc_range_search(const orc_index* ix, const float* query, uin
   return ORC_OK;
 }
 
+// Paged search (diskann/src/graph/search/paged.rs; index.rs:2080-2160), FullPrecision
+// accessor.  A session holds the resizable queue (capacity L + #start points, never
+// dropping), the visited set, the page cache and the running comparison / hop counters.
+struct orc_paged {
+  const orc_index* ix;
+  std::vector<float> query;
+  Queue best;
+  VisitedSet visited;
+  std::vector<std::pair<uint32_t, float>> computed;  // computed_result
+  size_t next = 0;                                    // next_result_index
+  uint32_t l_value = 0;
+  uint32_t cmps = 0, hops = 0;
+  orc_paged(const orc_index* x, size_t qcap, size_t vcap) : ix(x), best(qcap), visited(vcap) {}
+};
+
+// index.rs:2101-2160 `paged_search_with_init_ids`: the init ids (default: the start points)
+// go into the visited set, their neighbours are expanded through it and inserted in order;
+// the counters start at zero (search_internal then skips the start-point step because the
+// visited set is not empty, index.rs:1953-1963).
+extern "C" int32_t orc_paged_create(const orc_index* ix, const float* query, uint32_t l_value,
+                                    const uint32_t* init_ids, uint32_t n_init,
+                                    orc_paged** out) {
+  if (!ix || !query || !out) return ORC_ERR_INVALID_ARGUMENT;
+  const uint32_t n_start = ix->num_frozen;
+  auto* ps = new orc_paged(ix, (size_t)l_value + n_start,
+                           (size_t)std::ceil(1.1 * ix->max_degree * 1.3 * l_value));
+  ps->best.resizable = true;
+  ps->query.assign(query, query + ix->dim);
+  ps->l_value = l_value;
+  std::vector<uint32_t> init;
+  if (n_init) init.assign(init_ids, init_ids + n_init);
+  else
+    for (uint32_t s = 0; s < n_start; ++s) init.push_back(ix->num_points + s);
+  for (uint32_t id : init) ps->visited.insert(id);
+  Scorer score{ix, ps->query.data(), false, {}};
+  std::vector<std::pair<uint32_t, float>> neighbors;
+  for (uint32_t id : init) expand(ix, score, ps->visited, id, neighbors);
+  for (const auto& nb : neighbors) ps->best.insert(nb.first, nb.second);
+  ps->computed.assign(l_value, {0u, 0.0f});
+  ps->next = l_value;
+  *out = ps;
+  return ORC_OK;
+}
+
+// paged.rs:52-126 `next_page` with `filter_search_candidates` (paged.rs:128-151).
+extern "C" int32_t orc_paged_next(orc_paged* ps, uint32_t k, uint32_t* ids_out,
+                                  float* dists_out, uint32_t* count_out, orc_stats* stats) {
+  if (!ps) return ORC_ERR_INVALID_ARGUMENT;
+  if (k > ps->l_value || k == 0) return ORC_ERR_INVALID_ARGUMENT;
+  const orc_index* ix = ps->ix;
+  uint32_t n = 0;
+  const size_t available = ps->computed.size() > ps->next ? ps->computed.size() - ps->next : 0;
+  const size_t from_cache = std::min<size_t>(k, available);
+  for (size_t i = 0; i < from_cache; ++i) {
+    ids_out[n] = ps->computed[ps->next + i].first;
+    dists_out[n++] = ps->computed[ps->next + i].second;
+  }
+  ps->next += from_cache;
+  if (n < k) {
+    Scorer score{ix, ps->query.data(), false, {}};
+    search_loop(ix, score, ps->best, ps->visited, 1, ps->cmps, ps->hops);
+    std::vector<std::pair<uint32_t, float>> cand;
+    size_t total = 0;
+    for (size_t i = 0; i < ps->best.iter_len(); ++i) {
+      ++total;
+      if (ps->best.ids[i] < ix->num_points) {  // start points are ids N..N+F-1
+        cand.emplace_back(ps->best.ids[i], ps->best.dists[i]);
+        if (cand.size() >= k) break;
+      }
+    }
+    ps->best.drain_best(total);
+    ps->computed = cand;
+    ps->next = 0;
+    const size_t leftover = std::min<size_t>(k - n, cand.size());
+    for (size_t i = 0; i < leftover; ++i) {
+      ids_out[n] = cand[i].first;
+      dists_out[n++] = cand[i].second;
+    }
+    ps->next = leftover;
+  }
+  *count_out = n;
+  if (stats) {
+    stats->cmps = ps->cmps;
+    stats->hops = ps->hops;
+    stats->result_count = n;
+    stats->flags = 0;
+  }
+  return ORC_OK;
+}
+
+extern "C" void orc_paged_destroy(orc_paged* ps) { delete ps; }
+
 // One k-NN search.
 //
 // diskann/src/graph/search/knn_search.rs:178-216 `<Knn as Search>::search`: the queue
@@ -568,6 +676,131 @@ extern "C" int32_t orc_search(const orc_index* ix, int32_t strategy, const float
     stats->flags = 0;
   }
   return ORC_OK;
+}
+
+// diskann-inmem provider search (diskann-inmem/src/provider.rs:380-960).  Rows are the store's
+// slots: `dim` elements of `elem` then the one-byte tag (store.rs:150-260); a slot is
+// readable when its tag is >= 254 (tag.rs Tag::can_read).  FP32 and FP16 data are scored by
+// the FP32 restatement on the exact f32 values (the f32-by-f16 kernels, simd.rs:1121-1156,
+// 1878-1912, 2716-2747, run Strategy4x2 / Strategy2x4, which feed each accumulator the same
+// vectors in the same order as Strategy4x1 / Strategy2x4 over f32), so `ix->vectors` holds the
+// converted rows and `query` f32 values.  u8 / i8 data are scored in exact integers
+// (simd.rs:1192-1227, 1370-1405, 1947-1981, 2109-2145, 2790-2829, 2996-3035: i32 lanes, one
+// lossy conversion to f32 per sum), `query` then holds `dim` bytes.
+namespace {
+
+struct IntScorer {
+  const orc_index* ix;
+  const uint8_t* rows;
+  uint64_t row_stride;
+  const uint8_t* query;
+  bool is_signed;
+
+  int64_t at(const uint8_t* p, uint32_t i) const {
+    return is_signed ? (int64_t)(int8_t)p[i] : (int64_t)p[i];
+  }
+  float operator()(uint32_t id) const {
+    const uint8_t* y = rows + (uint64_t)id * row_stride;
+    int64_t xx = 0, yy = 0, xy = 0, l2 = 0;
+    for (uint32_t i = 0; i < ix->dim; ++i) {
+      const int64_t a = at(query, i), b = at(y, i);
+      xx += a * a;
+      yy += b * b;
+      xy += a * b;
+      l2 += (a - b) * (a - b);
+    }
+    // The i32 lanes wrap; the sums are converted with round-to-nearest-even.
+    auto lossy = [](int64_t v) { return (float)(int32_t)(uint32_t)(uint64_t)v; };
+    switch (ix->metric) {
+      case ORC_METRIC_L2: return lossy(l2);
+      case ORC_METRIC_INNER_PRODUCT: return -lossy(xy);
+      default: {  // Cosine; the integer layers map CosineNormalized to Cosine
+        const float nx = lossy(xx), ny = lossy(yy), pr = lossy(xy);
+        const float denom = std::sqrt(nx) * std::sqrt(ny);
+        if (nx < FLT_MIN || ny < FLT_MIN) return 1.0f;
+        return 1.0f - std::max(-1.0f, std::min(1.0f, pr / denom));
+      }
+    }
+  }
+};
+
+template <class Score>
+int32_t inmem_search(const orc_index* ix, const uint8_t* rows, uint64_t row_stride,
+                     uint32_t tag_offset, const uint64_t* ext, const Score& score, uint32_t k,
+                     uint32_t l, uint32_t beam_width, uint64_t* ids_out, float* dists_out,
+                     orc_stats* stats) {
+  const int32_t verr = orc_validate_knn(k, l, beam_width);
+  if (verr != ORC_OK) return verr;
+  auto readable = [&](uint32_t id) { return rows[(uint64_t)id * row_stride + tag_offset] >= 254; };
+  const uint32_t n_start = ix->num_frozen;
+  Queue best((size_t)l + n_start);
+  VisitedSet visited((size_t)std::ceil(1.1 * ix->max_degree * 1.3 * l));
+  uint32_t cmps = 0, hops = 0;
+  // start_point_distances (provider.rs:415-440): the frozen slots, always readable.
+  for (uint32_t s = 0; s < n_start; ++s) {
+    const uint32_t id = ix->num_points + s;
+    visited.insert(id);
+    best.insert(id, score(id));
+    cmps += 1;
+  }
+  std::vector<uint32_t> beam;
+  std::vector<std::pair<uint32_t, float>> neighbors;
+  while (best.has_notvisited()) {
+    beam.clear();
+    uint32_t node;
+    while (beam.size() < beam_width && best.closest_notvisited(&node)) beam.push_back(node);
+    neighbors.clear();
+    // expand_beam (provider.rs:443-478): retain(visited-set insert && in bounds), then score
+    // the slots whose tag is readable, in order; the others stay visited.
+    for (uint32_t n : beam) {
+      const uint32_t deg = ix->degrees[n];
+      const uint32_t* adj = ix->adjacency + (size_t)n * ix->adjacency_stride;
+      for (uint32_t t = 0; t < deg; ++t) {
+        const uint32_t id = adj[t];
+        if (visited.insert(id) && readable(id)) neighbors.emplace_back(id, score(id));
+      }
+    }
+    for (const auto& nb : neighbors) best.insert(nb.first, nb.second);
+    cmps += (uint32_t)neighbors.size();
+    hops += (uint32_t)beam.size();
+  }
+  // Translate (provider.rs:906-945): candidates with an external id, in order, up to k.
+  uint32_t count = 0;
+  for (size_t i = 0; i < best.iter_len() && count < k; ++i) {
+    const uint64_t e = ext[best.ids[i]];
+    if (e == ORC_NO_EXTERNAL_ID) continue;
+    ids_out[count] = e;
+    dists_out[count++] = best.dists[i];
+  }
+  for (uint32_t i = count; i < k; ++i) {
+    ids_out[i] = ORC_NO_EXTERNAL_ID;
+    dists_out[i] = INFINITY;
+  }
+  if (stats) {
+    stats->cmps = cmps;
+    stats->hops = hops;
+    stats->result_count = count;
+    stats->flags = 0;
+  }
+  return ORC_OK;
+}
+
+}  // namespace
+
+extern "C" int32_t orc_inmem_search(const orc_index* ix, int32_t elem, const uint8_t* rows,
+                                    uint64_t row_stride, const uint64_t* ext, const void* query,
+                                    uint32_t k, uint32_t l, uint32_t beam_width,
+                                    uint64_t* ids_out, float* dists_out, orc_stats* stats) {
+  const uint32_t eb = elem == ORC_ELEM_F32 ? 4u : (elem == ORC_ELEM_F16 ? 2u : 1u);
+  const uint32_t tag_offset = ix->dim * eb;
+  if (elem == ORC_ELEM_U8 || elem == ORC_ELEM_I8) {
+    const IntScorer score{ix, rows, row_stride, static_cast<const uint8_t*>(query), elem == ORC_ELEM_I8};
+    return inmem_search(ix, rows, row_stride, tag_offset, ext, score, k, l, beam_width, ids_out,
+                        dists_out, stats);
+  }
+  const Scorer score{ix, static_cast<const float*>(query), false, {}};
+  return inmem_search(ix, rows, row_stride, tag_offset, ext, score, k, l, beam_width, ids_out,
+                      dists_out, stats);
 }
 
 // Many queries on `num_threads` host threads.  Queries are split into contiguous ranges,

@@ -32,6 +32,9 @@ enum {
 };
 
 #define ORC_INVALID_ID 0xFFFFFFFFu
+#define ORC_NO_EXTERNAL_ID 0xFFFFFFFFFFFFFFFFull
+
+enum { ORC_ELEM_F32 = 0, ORC_ELEM_F16 = 1, ORC_ELEM_U8 = 2, ORC_ELEM_I8 = 3 };
 
 // An in-memory index: ids 0..num_points-1 are data, num_points..num_points+num_frozen-1
 // are frozen start points.  All arrays have num_points + num_frozen rows.
@@ -65,6 +68,16 @@ int32_t orc_validate_knn(uint32_t k, uint32_t l, uint32_t beam_width);
 int32_t orc_search(const orc_index* ix, int32_t strategy, const float* query, uint32_t k,
                    uint32_t l, uint32_t beam_width, uint32_t* ids_out, float* dists_out,
                    orc_stats* stats);
+int32_t orc_inmem_search(const orc_index* ix, int32_t elem, const uint8_t* rows,
+                         uint64_t row_stride, const uint64_t* ext, const void* query, uint32_t k,
+                         uint32_t l, uint32_t beam_width, uint64_t* ids_out, float* dists_out,
+                         orc_stats* stats);
+typedef struct orc_paged orc_paged;
+int32_t orc_paged_create(const orc_index* ix, const float* query, uint32_t l_value,
+                         const uint32_t* init_ids, uint32_t n_init, orc_paged** out);
+int32_t orc_paged_next(orc_paged* ps, uint32_t k, uint32_t* ids_out, float* dists_out,
+                       uint32_t* count_out, orc_stats* stats);
+void orc_paged_destroy(orc_paged* ps);
 int32_t orc_range_search(const orc_index* ix, const float* query, uint32_t starting_l,
                          uint32_t beam_width, float radius, float inner_radius,
                          float initial_slack, float range_slack, uint32_t max_returned,

@@ -106,6 +106,20 @@ def lib():
                 ctypes.POINTER(_Index), ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32,
                 ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_uint32,
                 ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+            L.orc_inmem_search.restype = ctypes.c_int32
+            L.orc_inmem_search.argtypes = [
+                ctypes.POINTER(_Index), ctypes.c_int32, ctypes.c_void_p, ctypes.c_uint64,
+                ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+            L.orc_paged_create.restype = ctypes.c_int32
+            L.orc_paged_create.argtypes = [ctypes.POINTER(_Index), ctypes.c_void_p, ctypes.c_uint32,
+                                           ctypes.c_void_p, ctypes.c_uint32,
+                                           ctypes.POINTER(ctypes.c_void_p)]
+            L.orc_paged_next.restype = ctypes.c_int32
+            L.orc_paged_next.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
+                                         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+            L.orc_paged_destroy.restype = None
+            L.orc_paged_destroy.argtypes = [ctypes.c_void_p]
             _lib = L
     return _lib
 
@@ -193,11 +207,68 @@ class OracleIndex:
         n = int(st[0]["result_count"])
         return ids[:n], dists[:n], st[0]
 
+    def inmem_search(self, elem, rows, external_ids, query, k, l, beam_width=1):
+        """diskann-inmem search of one query (provider.rs restated).  ``rows``: the store's
+        slots (uint8, element bytes then the tag); ``elem``: 0 f32, 1 f16, 2 u8, 3 i8; the
+        index's own vectors must hold the rows' f32 values.  ``query``: f32 values for f32 /
+        f16 data, the element bytes for u8 / i8.  Returns ``(external ids, dists, stats)``."""
+        rows = np.ascontiguousarray(rows, dtype=np.uint8)
+        ext = np.ascontiguousarray(external_ids, dtype=np.uint64)
+        if elem in (2, 3):
+            q = np.ascontiguousarray(np.ravel(query)).view(np.uint8).copy()
+        else:
+            q = np.ascontiguousarray(np.ravel(query), dtype=np.float32)
+        ids = np.empty(k, dtype=np.uint64)
+        dists = np.empty(k, dtype=np.float32)
+        st = np.zeros(1, dtype=STATS_DTYPE)
+        rc = lib().orc_inmem_search(ctypes.byref(self._s), elem, _ptr(rows), rows.shape[1],
+                                    _ptr(ext), _ptr(q), k, l, beam_width, _ptr(ids), _ptr(dists),
+                                    _ptr(st))
+        if rc != 0:
+            raise ValueError(f"oracle inmem search failed with status {rc}")
+        return ids, dists, st[0]
+
+    def paged_search(self, query, l_value, init_ids=None):
+        """Start a paged search of one query (paged.rs restated); returns an
+        :class:`OraclePagedSearch` whose ``next_page(k)`` yields ``(ids, dists, stats)``."""
+        return OraclePagedSearch(self, query, l_value, init_ids)
+
     def pq_table(self, query):
         q = np.ascontiguousarray(query, dtype=np.float32)
         out = np.empty((len(self.pq_offsets) - 1, 256), dtype=np.float32)
         lib().orc_pq_table(ctypes.byref(self._s), _ptr(q), _ptr(out))
         return out
+
+
+class OraclePagedSearch:
+    """One paged-search session (index.rs:2101-2160, paged.rs:52-151); stats are the
+    session's running comparison and hop counters."""
+
+    def __init__(self, index: "OracleIndex", query, l_value: int, init_ids=None):
+        self._index = index  # keeps the index arrays alive
+        q = np.ascontiguousarray(np.ravel(query), dtype=np.float32)
+        init = None if init_ids is None else np.ascontiguousarray(init_ids, dtype=np.uint32)
+        h = ctypes.c_void_p()
+        rc = lib().orc_paged_create(ctypes.byref(index._s), _ptr(q), l_value, _ptr(init),
+                                    0 if init is None else init.size, ctypes.byref(h))
+        if rc != 0:
+            raise ValueError(f"oracle paged search failed with status {rc}")
+        self._h = h
+
+    def next_page(self, k: int):
+        ids = np.empty(max(k, 1), dtype=np.uint32)
+        dists = np.empty(max(k, 1), dtype=np.float32)
+        n = np.zeros(1, dtype=np.uint32)
+        st = np.zeros(1, dtype=STATS_DTYPE)
+        rc = lib().orc_paged_next(self._h, k, _ptr(ids), _ptr(dists), _ptr(n), _ptr(st))
+        if rc != 0:
+            raise ValueError(f"oracle paged search failed with status {rc}")
+        return ids[: n[0]], dists[: n[0]], st[0]
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().orc_paged_destroy(self._h)
+            self._h = None
 
 
 def validate_knn(k: int, l: int, beam_width: int) -> int:

@@ -10,9 +10,9 @@ tests compare.  Run it from the repository root:
 
     python tests/golden/make_golden.py /path/to/reference
 
-It writes ``tests/golden/grid_search.json``, ``tests/golden/flat_knn_search.json`` and
+It writes ``tests/golden/grid_search.json``, ``tests/golden/flat_knn_search.json``,
 ``tests/golden/range_search.json`` (range_search.rs's baselines with the Range parameters of
-each case).
+each case) and ``tests/golden/paged_search.json`` (paged_search.rs's pages).
 """
 
 import json
@@ -30,6 +30,8 @@ RANGE_CASES = {
     "max_results_respected_means_no_second_round.json": (4, 1.0, 1.0),
     "max_results_respected_and_second_round_triggered.json": (5, 1.0, 1.0),
 }
+PAGED_DIR = "diskann/test/generated/graph/test/cases/paged_search"
+PAGED_FILES = ["basic_paged_search.json", "single_page.json", "small_page_size.json"]
 FLAT_DIR = "diskann/test/generated/flat/test/cases/flat_knn_search"
 GRID_FILES = ["search_1_100.json", "search_3_5.json", "search_4_4.json"]
 FLAT_FILES = ["search_1_100.json", "search_2_5.json", "search_3_4.json"]
@@ -105,7 +107,26 @@ def main(ref_root: str) -> None:
         )
     with open(os.path.join(out_dir, "range_search.json"), "w") as f:
         json.dump(rng, f, indent=1)
-    print(f"wrote {len(grid)} grid, {len(flat)} flat and {len(rng)} range cases to {out_dir}")
+    paged = []
+    for name in PAGED_FILES:
+        with open(os.path.join(ref_root, PAGED_DIR, name)) as f:
+            c = json.load(f)["payload"]
+        paged.append(
+            {
+                "source": f"{PAGED_DIR}/{name}",
+                "grid_dims": c["dims"],
+                "grid_size": c["grid_size"],
+                "query": c["query"],
+                "search_l": c["search_l"],
+                "page_size": c["page_size"],
+                "pages": c["pages"],
+                "total_results": c["total_results"],
+            }
+        )
+    with open(os.path.join(out_dir, "paged_search.json"), "w") as f:
+        json.dump(paged, f)
+    print(f"wrote {len(grid)} grid, {len(flat)} flat, {len(rng)} range and {len(paged)} paged "
+          f"cases to {out_dir}")
 
 
 if __name__ == "__main__":

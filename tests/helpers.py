@@ -59,3 +59,31 @@ def queries_like(vectors: np.ndarray, nq: int, seed: int, normalize: bool = Fals
     if normalize:
         q /= np.linalg.norm(q, axis=1, keepdims=True)
     return q.astype(np.float32)
+
+
+def inmem_fixture(elem: str, n: int, dim: int, seed: int, metric: int = 2,
+                  unreadable: float = 0.1, unmapped: float = 0.05, degree: int = 24):
+    """A diskann-inmem store: typed vectors (f32 / f16 / u8 / i8) from the mixture, random
+    graph, tags (a fraction of data slots not readable), external ids (a fraction unmapped,
+    the frozen slot never).  Returns (typed vectors, f32 values, adjacency, degrees, n, tags,
+    external ids)."""
+    v, adj, deg, n = random_index(n, dim, degree, seed, metric=metric, max_degree=degree + 7)
+    if elem == "f16":
+        typed = v.astype(np.float16)
+    elif elem == "u8":
+        typed = np.clip(np.rint(v), 0, 255).astype(np.uint8)
+    elif elem == "i8":
+        typed = (np.clip(np.rint(v), 0, 255) - 128).astype(np.int8)
+    else:
+        typed = v.astype(np.float32)
+    values = typed.astype(np.float32)
+    rng = np.random.default_rng(seed + 11)
+    total = typed.shape[0]
+    tags = np.full(total, 254, np.uint8)
+    tags[n:] = 255
+    bad = rng.random(n) < unreadable
+    tags[:n][bad] = rng.choice([0, 1, 2], size=int(bad.sum())).astype(np.uint8)
+    ext = (np.arange(total, dtype=np.uint64) * 10 + 1).astype(np.uint64)
+    ext[n:] = np.uint64(0xFFFFFFFFFFFFFFFF)
+    ext[:n][rng.random(n) < unmapped] = np.uint64(0xFFFFFFFFFFFFFFFF)
+    return typed, values, adj, deg, n, tags, ext

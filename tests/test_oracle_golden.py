@@ -268,3 +268,39 @@ def test_oracle_matches_range_golden(case):
     assert int(st["hops"]) == case["hops"]
     assert int(st["result_count"]) == case["result_count"]
     assert bool(int(st["flags"]) & 2) == case["second_round"]
+
+
+def _paged_cases():
+    with open(os.path.join(GOLDEN, "paged_search.json")) as f:
+        return json.load(f)
+
+
+def _oracle_pages(ix, case):
+    ps = ix.paged_search(np.array(case["query"], np.float32), case["search_l"])
+    pages = []
+    while True:
+        ids, dists, _ = ps.next_page(case["page_size"])
+        if len(ids) == 0:
+            break
+        pages.append([[int(i), float(x)] for i, x in zip(ids, dists)])
+    return pages, ps
+
+
+@pytest.mark.parametrize("case", _paged_cases(), ids=lambda c: c["source"].split("/")[-1][:-5])
+def test_oracle_matches_paged_golden(case):
+    """Every page of paged_search.rs's baselines (ids and distances, in order), until the
+    search is exhausted; then further calls stay empty."""
+    v, a, d, n = datasets.grid(case["grid_dims"], case["grid_size"])
+    ix = O.OracleIndex(v, a, d, n, O.METRIC_L2)
+    pages, ps = _oracle_pages(ix, case)
+    assert pages == case["pages"]
+    assert sum(len(p) for p in pages) == case["total_results"]
+    assert len(ps.next_page(case["page_size"])[0]) == 0
+
+
+def test_oracle_paged_errors():
+    v, a, d, n = datasets.grid(3, 5)
+    ps = O.OracleIndex(v, a, d, n, O.METRIC_L2).paged_search(np.full(3, 5.0, np.float32), 8)
+    for k in (0, 9):
+        with pytest.raises(ValueError):
+            ps.next_page(k)
