@@ -475,6 +475,115 @@ def cpu_baseline(data, strategy, l, threads, min_seconds=2.0, max_reps=5, nq=Non
     return total / el, reps, res
 
 
+def _median_time(fn, reps=3):
+    fn()  # warm-up
+    ts = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        fn()
+        ts.append(time.perf_counter() - t0)
+    return float(np.median(ts))
+
+
+def next_rows(data, threads, build=True):
+    """Throughput of the paths beside the k-NN search, on the same index and queries: range
+    search, paged search, the diskann-inmem provider (u8 and f16 rows of the same vectors),
+    and graph construction on a 100k-point prefix (GPU-searched batches vs host only).  Host
+    buffers through the C ABI (copies inside the timing), median of 3 after a warm-up; each
+    beside the oracle's single-thread timing on a sample."""
+    from diskann_b200 import (DiskANNIndex, FullPrecision, GpuProvider, InmemProvider, Knn,
+                              Metric, Range, graph)
+    from diskann_b200.index import inmem_rows
+    from oracle import oracle as orc
+
+    w = data["w"]
+    n, k = data["n"], w["k"]
+    q = data["queries"]
+    nq = q.shape[0]
+    out = {}
+    prov = GpuProvider(data["vectors"], data["adj"], data["deg"], n, Metric.L2)
+    idx = DiskANNIndex(prov)
+    o = oracle_index(data)
+    sample = min(300, nq)
+
+    # Range: radius = median distance of the 10th neighbour at L = 50.
+    _, d10, _ = idx.search(Knn(k, 50), FullPrecision(), q)
+    radius = float(np.median(d10[:, k - 1]))
+    rp = Range(50, radius)
+    res = {}
+    t = _median_time(lambda: res.__setitem__("r", idx.range_search(rp, q, capacity=2000)))
+    counts = res["r"][1]["result_count"]
+    t0 = time.perf_counter()
+    for i in range(sample):
+        o.range_search(q[i], 50, radius, capacity=2000)
+    cpu = sample / (time.perf_counter() - t0)
+    out["range"] = {"qps": round(nq / t, 1), "cpu_qps": round(cpu, 1), "cpu_cores": 1,
+                    "starting_l": 50, "radius": round(radius, 3),
+                    "mean_results": round(float(counts.mean()), 2),
+                    "second_round": round(float((res["r"][1]["flags"] & 2).astype(bool).mean()), 3)}
+
+    # Paged: one session per query, l_value 50, three pages of 10.
+    def paged():
+        ps = idx.paged_search(q, 50)
+        for _ in range(3):
+            ps.next_page(k)
+        ps.close()
+    t = _median_time(paged)
+    t0 = time.perf_counter()
+    for i in range(sample // 3):
+        ops = o.paged_search(q[i], 50)
+        for _ in range(3):
+            ops.next_page(k)
+    cpu = 3 * (sample // 3) / (time.perf_counter() - t0)
+    out["paged"] = {"pages_per_s": round(3 * nq / t, 1), "cpu_pages_per_s": round(cpu, 1),
+                    "cpu_cores": 1, "l_value": 50, "page_size": k, "pages": 3}
+    prov.close()
+
+    # diskann-inmem provider: the same graph over u8 / f16 rows, all slots readable.
+    total = data["vectors"].shape[0]
+    tags = np.full(total, 254, np.uint8)
+    tags[n:] = 255
+    ext = np.arange(total, dtype=np.uint64)
+    ext[n:] = np.uint64(0xFFFFFFFFFFFFFFFF)
+    for name, typed, code in (("inmem_u8", np.clip(np.rint(data["vectors"]), 0, 255).astype(np.uint8), 2),
+                              ("inmem_f16", data["vectors"].astype(np.float16), 1)):
+        ip = InmemProvider(typed, data["adj"], data["deg"], n, tags, ext, Metric.L2)
+        qt = (np.clip(np.rint(q), 0, 255).astype(np.uint8) if code == 2 else q.astype(np.float16))
+        res = {}
+        t = _median_time(lambda: res.__setitem__("r", ip.search(Knn(k, 50), qt)))
+        recall = float(np.mean([len(set(res["r"][0][i].tolist()) & set(data["gt"][i].tolist())) / k
+                                for i in range(nq)]))
+        ip.close()
+        oi = orc.OracleIndex(typed.astype(np.float32), data["adj"], data["deg"], n, orc.METRIC_L2)
+        rows = inmem_rows(typed, tags)
+        t0 = time.perf_counter()
+        for i in range(sample):
+            oi.inmem_search(code, rows, ext, qt[i] if code == 2 else qt[i].astype(np.float32), k, 50)
+        cpu = sample / (time.perf_counter() - t0)
+        out[name] = {"qps": round(nq / t, 1), "cpu_qps": round(cpu, 1), "cpu_cores": 1, "L": 50,
+                     "recall_at_10": round(recall, 4)}
+
+    if not build:
+        return out
+    # Graph construction on a 100k-point prefix: GPU-searched batches vs host threads only
+    # (the same graph, by construction).
+    sub = data["vectors"][: min(100_000, n)]
+    res = {}
+    t0 = time.perf_counter()
+    res["g"] = graph.build_vamana(sub, pruned_degree=w["R"], l_build=w["l_build"],
+                                  alpha=w["alpha"], device=0)
+    t_gpu = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    res["h"] = graph.build_vamana(sub, pruned_degree=w["R"], l_build=w["l_build"],
+                                  alpha=w["alpha"])
+    t_host = time.perf_counter() - t0
+    same = bool(np.array_equal(res["g"][2], res["h"][2]) and np.array_equal(res["g"][1], res["h"][1]))
+    out["build_100k"] = {"gpu_assisted_s": round(t_gpu, 2), "host_s": round(t_host, 2),
+                         "host_threads": threads, "points": int(sub.shape[0]),
+                         "identical_graph": same}
+    return out
+
+
 def cpu_model():
     try:
         with open("/proc/cpuinfo") as f:
@@ -533,11 +642,17 @@ def config_of(w, name, l, strategy):
 
 
 def profile_case(args):
-    """Two searches of the workload's query batch with one strategy and L (for ncu -s 1 -c 1)."""
+    """Two searches of the workload's query batch with one strategy and L (for ncu -s 1 -c 1),
+    or with ``--profile next`` the range / paged / inmem part of the next-rows section."""
     import torch
 
     from diskann_b200 import DiskANNIndex, GpuProvider, Knn, Metric
 
+    if args.profile == "next":
+        data = prepare(args.workload, 0, args.cache)
+        torch.cuda.set_device(0)
+        log(f"[profile] next rows {next_rows(data, os.cpu_count() or 1, build=False)}")
+        return 0
     name, l = args.profile.split(":")
     data = prepare(args.workload, 0, args.cache)
     w = data["w"]
@@ -568,9 +683,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--serve-seconds", type=float, default=1.0)
+    ap.add_argument("--no-next-rows", action="store_true",
+                    help="skip the range / paged / inmem / build throughput section")
     ap.add_argument("--profile", default=None, metavar="STRATEGY:L",
                     help="profiling case for ncu: upload the workload's index and run two "
-                         "batched searches (warm-up, profiled), no timing, no JSON line")
+                         "batched searches (warm-up, profiled), no timing, no JSON line; "
+                         "'next' runs the range / paged / inmem measurements instead")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -651,6 +769,9 @@ def main():
             "gpu_launches": r["gpu_launches"], "roofline": r["roofline"], "cpu_baseline": cpu,
             "clocks": r["clocks"], "search_stats": r["stats"],
         }
+        if world == 1 and not args.no_next_rows:
+            line["next_rows"] = next_rows(data, threads)
+            log(f"[ours] next rows {line['next_rows']}")
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

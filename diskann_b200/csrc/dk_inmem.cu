@@ -79,29 +79,48 @@ __global__ void __launch_bounds__(NT) k_inmem(const SearchParams P, const Transl
   }
 }
 
+// Launches the kernel, or with `occupancy` set only reports its resident CTAs per SM.
 template <int METRIC, int MODE, int DIM>
 cudaError_t launch_inmem(const SearchParams& P, const TranslateOut& T, uint32_t grid,
-                         cudaStream_t stream) {
+                         cudaStream_t stream, int* occupancy) {
   auto k = k_inmem<kCtaThreads, METRIC, MODE, DIM>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P.smem_bytes);
   if (e != cudaSuccess) return e;
+  if (occupancy)
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occupancy, k, kCtaThreads, P.smem_bytes);
   k<<<grid, kCtaThreads, P.smem_bytes, stream>>>(P, T);
   return cudaGetLastError();
 }
 
 template <int METRIC>
 cudaError_t inmem_modes(int32_t elem, const SearchParams& P, const TranslateOut& T,
-                        uint32_t grid, cudaStream_t stream) {
+                        uint32_t grid, cudaStream_t stream, int* occupancy) {
   const bool d128 = P.dim == 128;
   switch (elem) {
     case DK_ELEM_F32:
-      return d128 ? launch_inmem<METRIC, kModeFP32, 128>(P, T, grid, stream)
-                  : launch_inmem<METRIC, kModeFP32, 0>(P, T, grid, stream);
+      return d128 ? launch_inmem<METRIC, kModeFP32, 128>(P, T, grid, stream, occupancy)
+                  : launch_inmem<METRIC, kModeFP32, 0>(P, T, grid, stream, occupancy);
     case DK_ELEM_F16:
-      return d128 ? launch_inmem<METRIC, kModeF16, 128>(P, T, grid, stream)
-                  : launch_inmem<METRIC, kModeF16, 0>(P, T, grid, stream);
-    case DK_ELEM_U8: return launch_inmem<METRIC, kModeU8, 0>(P, T, grid, stream);
-    default: return launch_inmem<METRIC, kModeI8, 0>(P, T, grid, stream);
+      return d128 ? launch_inmem<METRIC, kModeF16, 128>(P, T, grid, stream, occupancy)
+                  : launch_inmem<METRIC, kModeF16, 0>(P, T, grid, stream, occupancy);
+    case DK_ELEM_U8: return launch_inmem<METRIC, kModeU8, 0>(P, T, grid, stream, occupancy);
+    default: return launch_inmem<METRIC, kModeI8, 0>(P, T, grid, stream, occupancy);
+  }
+}
+
+// u8 / i8 with CosineNormalized score as cosine (layers/full.rs:458-470, 487-492).
+cudaError_t inmem_dispatch(const dk_index* ix, const SearchParams& P, const TranslateOut& T,
+                           uint32_t grid, cudaStream_t stream, int* occupancy) {
+  const int32_t elem = ix->elem;
+  const bool int_elem = elem == DK_ELEM_U8 || elem == DK_ELEM_I8;
+  switch (ix->metric) {
+    case DK_METRIC_L2: return inmem_modes<DK_METRIC_L2>(elem, P, T, grid, stream, occupancy);
+    case DK_METRIC_INNER_PRODUCT:
+      return inmem_modes<DK_METRIC_INNER_PRODUCT>(elem, P, T, grid, stream, occupancy);
+    case DK_METRIC_COSINE: return inmem_modes<DK_METRIC_COSINE>(elem, P, T, grid, stream, occupancy);
+    default:
+      return int_elem ? inmem_modes<DK_METRIC_COSINE>(elem, P, T, grid, stream, occupancy)
+                      : inmem_modes<DK_METRIC_COSINE_NORMALIZED>(elem, P, T, grid, stream, occupancy);
   }
 }
 
@@ -282,9 +301,13 @@ extern "C" int32_t dk_inmem_search(dk_index* ix, const void* queries, uint64_t q
   cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ix->device);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ix->device);
   if (P.smem_bytes > (uint32_t)max_optin) return fail(DK_ERR_UNSUPPORTED, "search state does not fit in shared memory (L too large)");
+  // Persistent grid: every resident CTA (occupancy) owns a bitmap, within 512 MiB of bitmaps.
   const uint32_t words = (ix->n + ix->f + 31u) / 32u;
   const uint64_t per = (uint64_t)words * 4u;
-  uint32_t grid = std::min<uint32_t>(nq, 2u * (uint32_t)std::max(1, sms));
+  int occ = 0;
+  cudaError_t eo = inmem_dispatch(ix, P, TranslateOut{}, 0, nullptr, &occ);
+  if (eo != cudaSuccess) return fail(DK_ERR_CUDA, std::string("inmem occupancy: ") + cudaGetErrorString(eo));
+  uint32_t grid = std::min<uint32_t>(nq, (uint32_t)std::max(1, occ) * (uint32_t)std::max(1, sms));
   if (per * grid > (512ull << 20)) grid = (uint32_t)std::max<uint64_t>(1, (512ull << 20) / per);
   const size_t qbytes = qh.size() * 4, obytes = (size_t)nq * k;
   const size_t o_ids = (qbytes + 255) / 256 * 256;
@@ -308,19 +331,7 @@ extern "C" int32_t dk_inmem_search(dk_index* ix, const void* queries, uint64_t q
   P.bitmap = reinterpret_cast<uint32_t*>(buf + o_bm);
   P.bitmap_words = words;
   const TranslateOut T{ix->ext, reinterpret_cast<uint64_t*>(buf + o_ids)};
-  if (e == cudaSuccess) {
-    // u8 / i8 with CosineNormalized score as cosine (layers/full.rs:458-470, 487-492).
-    const bool int_elem = elem == DK_ELEM_U8 || elem == DK_ELEM_I8;
-    switch (ix->metric) {
-      case DK_METRIC_L2: e = inmem_modes<DK_METRIC_L2>(elem, P, T, grid, s); break;
-      case DK_METRIC_INNER_PRODUCT: e = inmem_modes<DK_METRIC_INNER_PRODUCT>(elem, P, T, grid, s); break;
-      case DK_METRIC_COSINE: e = inmem_modes<DK_METRIC_COSINE>(elem, P, T, grid, s); break;
-      default:
-        e = int_elem ? inmem_modes<DK_METRIC_COSINE>(elem, P, T, grid, s)
-                     : inmem_modes<DK_METRIC_COSINE_NORMALIZED>(elem, P, T, grid, s);
-        break;
-    }
-  }
+  if (e == cudaSuccess) e = inmem_dispatch(ix, P, T, grid, s, nullptr);
   if (e == cudaSuccess) e = cudaMemcpyAsync(ids, buf + o_ids, obytes * 8, cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(dists, buf + o_d, obytes * 4, cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess && stats)

@@ -308,25 +308,28 @@ __global__ void __launch_bounds__(NT) k_paged(const SearchParams P, const PagedP
   }
 }
 
+// Launches the kernel, or with `occupancy` set only reports its resident CTAs per SM.
 template <int METRIC, int DIM>
 cudaError_t launch_paged(const SearchParams& P, const PagedParams& G, bool init, uint32_t grid,
-                         cudaStream_t stream) {
+                         cudaStream_t stream, int* occupancy) {
   auto k = init ? k_paged<kCtaThreads, METRIC, DIM, true> : k_paged<kCtaThreads, METRIC, DIM, false>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P.smem_bytes);
   if (e != cudaSuccess) return e;
+  if (occupancy)
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occupancy, k, kCtaThreads, P.smem_bytes);
   k<<<grid, kCtaThreads, P.smem_bytes, stream>>>(P, G);
   return cudaGetLastError();
 }
 
 template <int METRIC>
 cudaError_t paged_dims(const SearchParams& P, const PagedParams& G, bool init, uint32_t grid,
-                       cudaStream_t stream) {
+                       cudaStream_t stream, int* occupancy) {
   switch (P.dim) {
-    case 96: return launch_paged<METRIC, 96>(P, G, init, grid, stream);
-    case 128: return launch_paged<METRIC, 128>(P, G, init, grid, stream);
-    case 384: return launch_paged<METRIC, 384>(P, G, init, grid, stream);
-    case 768: return launch_paged<METRIC, 768>(P, G, init, grid, stream);
-    default: return launch_paged<METRIC, 0>(P, G, init, grid, stream);
+    case 96: return launch_paged<METRIC, 96>(P, G, init, grid, stream, occupancy);
+    case 128: return launch_paged<METRIC, 128>(P, G, init, grid, stream, occupancy);
+    case 384: return launch_paged<METRIC, 384>(P, G, init, grid, stream, occupancy);
+    case 768: return launch_paged<METRIC, 768>(P, G, init, grid, stream, occupancy);
+    default: return launch_paged<METRIC, 0>(P, G, init, grid, stream, occupancy);
   }
 }
 
@@ -351,13 +354,16 @@ struct dk_paged {
 
 namespace {
 
-cudaError_t paged_launch(dk_paged* ps, bool init) {
+cudaError_t paged_launch(dk_paged* ps, bool init, int* occupancy = nullptr) {
   switch (ps->ix->metric) {
-    case DK_METRIC_L2: return paged_dims<DK_METRIC_L2>(ps->P, ps->G, init, ps->grid, ps->stream);
+    case DK_METRIC_L2:
+      return paged_dims<DK_METRIC_L2>(ps->P, ps->G, init, ps->grid, ps->stream, occupancy);
     case DK_METRIC_INNER_PRODUCT:
-      return paged_dims<DK_METRIC_INNER_PRODUCT>(ps->P, ps->G, init, ps->grid, ps->stream);
-    case DK_METRIC_COSINE: return paged_dims<DK_METRIC_COSINE>(ps->P, ps->G, init, ps->grid, ps->stream);
-    default: return paged_dims<DK_METRIC_COSINE_NORMALIZED>(ps->P, ps->G, init, ps->grid, ps->stream);
+      return paged_dims<DK_METRIC_INNER_PRODUCT>(ps->P, ps->G, init, ps->grid, ps->stream, occupancy);
+    case DK_METRIC_COSINE:
+      return paged_dims<DK_METRIC_COSINE>(ps->P, ps->G, init, ps->grid, ps->stream, occupancy);
+    default:
+      return paged_dims<DK_METRIC_COSINE_NORMALIZED>(ps->P, ps->G, init, ps->grid, ps->stream, occupancy);
   }
 }
 
@@ -442,9 +448,15 @@ extern "C" int32_t dk_paged_search_create(dk_index* ix, const float* queries,
   G.stats = reinterpret_cast<dk_search_stats*>(b + o_st);
   G.init_ids = n_init ? reinterpret_cast<const uint32_t*>(b + o_init) : nullptr;
   G.n_init = n_init;
-  int sms = 0;
+  // Persistent grid of every resident CTA (each session owns its bitmap, so no cap here).
+  int sms = 0, occ = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ix->device);
-  ps->grid = std::min<uint32_t>(nq, 4u * (uint32_t)std::max(1, sms));
+  e = paged_launch(ps, false, &occ);
+  if (e != cudaSuccess) {
+    paged_release(ps);
+    return fail(DK_ERR_CUDA, std::string("paged occupancy: ") + cudaGetErrorString(e));
+  }
+  ps->grid = std::min<uint32_t>(nq, (uint32_t)std::max(1, occ) * (uint32_t)std::max(1, sms));
   if (query_stride == ix->dim)
     e = cudaMemcpyAsync(b + o_query, queries, (size_t)nq * ix->dim * 4, cudaMemcpyHostToDevice, ps->stream);
   else

@@ -155,25 +155,38 @@ __global__ void __launch_bounds__(NT) k_range_cta(const SearchParams P, const Ra
   }
 }
 
+// Launches the kernel, or with `occupancy` set only reports its resident CTAs per SM.
 template <int METRIC, int DIM>
 cudaError_t launch_range(const SearchParams& P, const RangeParams& R, uint32_t grid,
-                         cudaStream_t stream) {
+                         cudaStream_t stream, int* occupancy) {
   auto k = k_range_cta<kCtaThreads, METRIC, DIM>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P.smem_bytes);
   if (e != cudaSuccess) return e;
+  if (occupancy)
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occupancy, k, kCtaThreads, P.smem_bytes);
   k<<<grid, kCtaThreads, P.smem_bytes, stream>>>(P, R);
   return cudaGetLastError();
 }
 
 template <int METRIC>
 cudaError_t range_dims(const SearchParams& P, const RangeParams& R, uint32_t grid,
-                       cudaStream_t stream) {
+                       cudaStream_t stream, int* occupancy) {
   switch (P.dim) {
-    case 96: return launch_range<METRIC, 96>(P, R, grid, stream);
-    case 128: return launch_range<METRIC, 128>(P, R, grid, stream);
-    case 384: return launch_range<METRIC, 384>(P, R, grid, stream);
-    case 768: return launch_range<METRIC, 768>(P, R, grid, stream);
-    default: return launch_range<METRIC, 0>(P, R, grid, stream);
+    case 96: return launch_range<METRIC, 96>(P, R, grid, stream, occupancy);
+    case 128: return launch_range<METRIC, 128>(P, R, grid, stream, occupancy);
+    case 384: return launch_range<METRIC, 384>(P, R, grid, stream, occupancy);
+    case 768: return launch_range<METRIC, 768>(P, R, grid, stream, occupancy);
+    default: return launch_range<METRIC, 0>(P, R, grid, stream, occupancy);
+  }
+}
+
+cudaError_t range_dispatch(int32_t metric, const SearchParams& P, const RangeParams& R,
+                           uint32_t grid, cudaStream_t stream, int* occupancy) {
+  switch (metric) {
+    case DK_METRIC_L2: return range_dims<DK_METRIC_L2>(P, R, grid, stream, occupancy);
+    case DK_METRIC_INNER_PRODUCT: return range_dims<DK_METRIC_INNER_PRODUCT>(P, R, grid, stream, occupancy);
+    case DK_METRIC_COSINE: return range_dims<DK_METRIC_COSINE>(P, R, grid, stream, occupancy);
+    default: return range_dims<DK_METRIC_COSINE_NORMALIZED>(P, R, grid, stream, occupancy);
   }
 }
 
@@ -225,10 +238,13 @@ int32_t launch_range_search(dk_index* ix, const float* queries, uint64_t qstride
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ix->device);
   if (P.smem_bytes > (uint32_t)max_optin)
     return fail(DK_ERR_UNSUPPORTED, "search state does not fit in shared memory (starting_l too large)");
-  // One exact bitmap over all ids per CTA; up to two CTAs per SM, within 512 MiB.
+  // One exact bitmap over all ids per resident CTA (occupancy), within 512 MiB.
   const uint32_t words = (ix->n + ix->f + 31u) / 32u;
   const uint64_t per = (uint64_t)words * 4u;
-  uint32_t grid = std::min<uint32_t>(nq, 2u * (uint32_t)std::max(1, sms));
+  int occ = 0;
+  const cudaError_t eo = range_dispatch(ix->metric, P, R, 0, nullptr, &occ);
+  if (eo != cudaSuccess) return fail(DK_ERR_CUDA, std::string("range occupancy: ") + cudaGetErrorString(eo));
+  uint32_t grid = std::min<uint32_t>(nq, (uint32_t)std::max(1, occ) * (uint32_t)std::max(1, sms));
   if (per * grid > (512ull << 20)) grid = (uint32_t)std::max<uint64_t>(1, (512ull << 20) / per);
   unsigned char* scratch = nullptr;
   cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&scratch), per * grid, ix->pool, stream);
@@ -236,12 +252,7 @@ int32_t launch_range_search(dk_index* ix, const float* queries, uint64_t qstride
     return fail(DK_ERR_OUT_OF_MEMORY, std::string("range scratch: ") + cudaGetErrorString(e));
   P.bitmap = reinterpret_cast<uint32_t*>(scratch);
   P.bitmap_words = words;
-  switch (ix->metric) {
-    case DK_METRIC_L2: e = range_dims<DK_METRIC_L2>(P, R, grid, stream); break;
-    case DK_METRIC_INNER_PRODUCT: e = range_dims<DK_METRIC_INNER_PRODUCT>(P, R, grid, stream); break;
-    case DK_METRIC_COSINE: e = range_dims<DK_METRIC_COSINE>(P, R, grid, stream); break;
-    default: e = range_dims<DK_METRIC_COSINE_NORMALIZED>(P, R, grid, stream); break;
-  }
+  e = range_dispatch(ix->metric, P, R, grid, stream, nullptr);
   cudaFreeAsync(scratch, stream);
   if (e != cudaSuccess) return fail(DK_ERR_CUDA, std::string("range launch: ") + cudaGetErrorString(e));
   return DK_OK;

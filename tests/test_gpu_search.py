@@ -176,17 +176,19 @@ def test_k_equals_l_and_small_graph(kernel):
                     orc.search(q, k, l, 1, O.STRATEGY_FULL_PRECISION))
 
 
-def test_device_entry_point_matches_host_entry_point():
+@pytest.mark.parametrize("nq", [100, 9000])
+def test_device_entry_point_matches_host_entry_point(nq):
+    """The host entry point returns exactly what the device entry point returns."""
     import torch
 
-    v, a, d, n = random_index(2000, 64, 16, seed=71, max_degree=20)
-    q = queries_like(v[:n], 100, seed=72)
+    v, a, d, n = random_index(12000, 64, 16, seed=71, max_degree=20)
+    q = queries_like(v[:n], nq, seed=72)
     idx = DiskANNIndex(GpuProvider(v, a, d, n, Metric.L2))
     hi, hd, hs = idx.search(Knn(10, 50), FullPrecision(), q)
     dq = torch.from_numpy(q).cuda()
-    ids = torch.empty((100, 10), dtype=torch.int32, device="cuda")
-    dists = torch.empty((100, 10), dtype=torch.float32, device="cuda")
-    st = torch.empty((100, 4), dtype=torch.int32, device="cuda")
+    ids = torch.empty((nq, 10), dtype=torch.int32, device="cuda")
+    dists = torch.empty((nq, 10), dtype=torch.float32, device="cuda")
+    st = torch.empty((nq, 4), dtype=torch.int32, device="cuda")
     idx.search_device(Knn(10, 50), FullPrecision(), dq, ids, dists, st)
     torch.cuda.synchronize()
     np.testing.assert_array_equal(ids.cpu().numpy().view(np.uint32), hi)
