@@ -363,33 +363,134 @@ int32_t build_impl(const float* vectors, uint64_t stride, uint32_t num_points, u
 
   std::vector<std::vector<uint32_t>> out;
   std::vector<uint32_t> changed;
+  const dk_build_prune_cfg cfg{B.p.alpha, B.p.pruned_degree, B.p.max_occlusion,
+                               B.occluding ? 1u : 0u};
+  // While batches run on the GPU, the device adjacency is the graph and B.adj is stale until
+  // it is read back; host batches keep B.adj current and push their changed rows.
+  bool device_graph = false;
+  auto pull_graph = [&]() -> int32_t {
+    if (!device_graph) return DK_OK;
+    device_graph = false;
+    return dk_build_gpu_get_rows(gpu, B.adj);
+  };
+  // Back-edge grouping by target (sources in point order), reused across batches.
+  std::vector<uint32_t> group_of(total, 0xFFFFFFFFu), g_targets, g_off, g_src, g_fill;
   uint32_t start = 0, bsize = 1;
   while (start < num_points) {
     const uint32_t end = std::min<uint32_t>(num_points, start + bsize);
     const uint32_t cnt = end - start;
     out.assign(cnt, {});
-    // The visited search record of every point of the batch against the graph before the
-    // batch: from the GPU for large batches (same search, bit-exact), else on the host.
-    const uint32_t* rec_ids = nullptr;
-    const float* rec_d = nullptr;
-    const uint32_t* hops = nullptr;
-    uint32_t rec_cap = 0;
     if (gpu && cnt >= kGpuMinBatch) {
-      const int32_t rc = dk_build_gpu_search(gpu, start, cnt, &rec_ids, &rec_d, &hops, &rec_cap);
+      // GPU batch: search, prune each point from its record, append and re-prune the back
+      // edges, all on the device graph; the host only groups the back edges.
+      device_graph = true;
+      const uint32_t *rec_ids = nullptr, *hops = nullptr, *fo = nullptr, *fc = nullptr;
+      const float* rec_d = nullptr;
+      uint32_t rec_cap = 0;
+      int32_t rc = dk_build_gpu_search(gpu, start, cnt, false, &rec_ids, &rec_d, &hops, &rec_cap);
+      if (rc == DK_OK) rc = dk_build_gpu_prune_forward(gpu, cnt, cfg, &fo, &fc);
+      if (rc != DK_OK) return rc;
+      std::vector<uint32_t> host_points;
+      for (uint32_t i = 0; i < cnt; ++i) {
+        if (fc[i] == 0xFFFFFFFFu) host_points.push_back(i);
+        else out[i].assign(fo + (size_t)i * B.p.pruned_degree, fo + (size_t)i * B.p.pruned_degree + fc[i]);
+      }
+      if (!host_points.empty()) {
+        // Records that overflowed: search and prune on the host against the graph before the
+        // batch (the device graph is unchanged so far in this batch).
+        rc = dk_build_gpu_get_rows(gpu, B.adj);
+        if (rc != DK_OK) return rc;
+        parallel_for(threads, host_points.size(), [&](uint64_t h, uint32_t w) {
+          const uint32_t i = host_points[h];
+          BuildScratch& S = scratch[w];
+          B.search(start + i, S);
+          std::vector<Candidate> pool = S.visited_record;
+          pool.erase(std::remove_if(pool.begin(), pool.end(),
+                                    [&](const Candidate& c) { return c.id == start + i; }),
+                     pool.end());
+          Builder::sort_pool(pool, B.p.max_occlusion);
+          B.occlude(start + i, pool, out[i]);
+        });
+      }
+      changed.clear();
+      for (uint32_t i = 0; i < cnt; ++i) {
+        B.adj[start + i] = out[i];
+        changed.push_back(start + i);
+      }
+      rc = dk_build_gpu_set_rows(gpu, changed.data(), (uint32_t)changed.size(), B.adj);
+      if (rc != DK_OK) return rc;
+      // Group the back edges by target with a counting pass; sources stay in point order.
+      g_targets.clear();
+      for (uint32_t i = 0; i < cnt; ++i)
+        for (uint32_t j = 0; j < out[i].size() && j < p.max_backedges; ++j) {
+          const uint32_t t = out[i][j];
+          if (group_of[t] == 0xFFFFFFFFu) {
+            group_of[t] = (uint32_t)g_targets.size();
+            g_targets.push_back(t);
+            g_off.push_back(0);
+          }
+          ++g_off[group_of[t]];
+        }
+      const uint32_t groups = (uint32_t)g_targets.size();
+      g_off.resize(groups + 1);
+      uint32_t max_group = 0, acc = 0;
+      for (uint32_t gi = 0; gi < groups; ++gi) {
+        const uint32_t c = g_off[gi];
+        max_group = std::max(max_group, c);
+        g_off[gi] = acc;
+        acc += c;
+      }
+      g_off[groups] = acc;
+      g_src.resize(acc);
+      g_fill.assign(g_off.begin(), g_off.end() - 1);
+      for (uint32_t i = 0; i < cnt; ++i)
+        for (uint32_t j = 0; j < out[i].size() && j < p.max_backedges; ++j)
+          g_src[g_fill[group_of[out[i][j]]]++] = start + i;
+      std::vector<uint32_t> oversize;
+      rc = dk_build_gpu_backedges(gpu, g_targets.data(), g_off.data(), g_src.data(), groups,
+                                  max_group, cfg, oversize);
+      if (rc != DK_OK) return rc;
+      // Lists too long for the device pool: append and prune on the host, write back.
+      for (uint32_t gi : oversize) {
+        const uint32_t target = g_targets[gi];
+        std::vector<uint32_t> lst;
+        rc = dk_build_gpu_get_row(gpu, target, lst);
+        if (rc != DK_OK) return rc;
+        bool added = false;
+        for (uint32_t e = g_off[gi]; e < g_off[gi + 1]; ++e)
+          if (std::find(lst.begin(), lst.end(), g_src[e]) == lst.end()) {
+            lst.push_back(g_src[e]);
+            added = true;
+          }
+        if (!added) continue;
+        if (lst.size() > p.max_degree) {
+          std::vector<Candidate> pool;
+          for (uint32_t id : lst)
+            if (id != target) pool.push_back({id, B.dist(target, id)});
+          Builder::sort_pool(pool, B.p.max_occlusion);
+          std::vector<uint32_t> pruned;
+          B.occlude(target, pool, pruned);
+          lst = pruned;
+        }
+        B.adj[target] = lst;
+        rc = dk_build_gpu_set_rows(gpu, &target, 1, B.adj);
+        if (rc != DK_OK) return rc;
+      }
+      for (uint32_t t : g_targets) group_of[t] = 0xFFFFFFFFu;
+      g_off.clear();
+      start = end;
+      bsize = std::min<uint32_t>(bsize * 2, B.p.max_batch);
+      continue;
+    }
+    if (gpu) {
+      const int32_t rc = pull_graph();
       if (rc != DK_OK) return rc;
     }
     parallel_for(threads, cnt, [&](uint64_t i, uint32_t w) {
       const uint32_t id = start + (uint32_t)i;
       BuildScratch& S = scratch[w];
-      std::vector<Candidate> pool;
-      if (rec_ids && hops[i] <= rec_cap) {
-        pool.reserve(hops[i]);
-        for (uint32_t h = 0; h < hops[i]; ++h)
-          pool.push_back({rec_ids[(size_t)i * rec_cap + h], rec_d[(size_t)i * rec_cap + h]});
-      } else {
-        B.search(id, S);
-        pool = S.visited_record;
-      }
+      B.search(id, S);
+      std::vector<Candidate> pool = S.visited_record;
       pool.erase(std::remove_if(pool.begin(), pool.end(),
                                 [&](const Candidate& c) { return c.id == id; }),
                  pool.end());
@@ -454,6 +555,10 @@ int32_t build_impl(const float* vectors, uint64_t stride, uint32_t num_points, u
     }
     start = end;
     bsize = std::min<uint32_t>(bsize * 2, B.p.max_batch);
+  }
+  if (gpu) {
+    const int32_t rc = pull_graph();
+    if (rc != DK_OK) return rc;
   }
   for (uint32_t i = 0; i < total; ++i) {
     const auto& lst = B.adj[i];
