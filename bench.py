@@ -48,9 +48,31 @@ WORKLOADS = {
                    alpha=1.2, pq_chunks=32, pq_train=100_000, k=10,
                    l_sweep=[50, 75, 100, 150, 200, 250, 300, 400],
                    strategies=["fp32", "bf16", "fp8", "hybrid"], seed=0xD15CA77 + 11),
+    # The cosine / inner-product shape with BF16 scoring: 1M x 768, isotropic Gaussian rows
+    # L2-normalised, inner product.
+    "ip768": dict(n=1_000_000, dim=768, normalized=True, metric=1, comps=0, sigma=0.0,
+                  nq=10_000, R=64, l_build=128, alpha=1.2, pq_chunks=0, pq_train=0, k=10,
+                  l_sweep=[128, 192, 256], strategies=["fp32", "bf16", "fp8"],
+                  seed=0xD15CA77 + 3),
+    # The same rows under CosineNormalized (1 - dot: the inner-product ranking on normalised
+    # rows, with the triangle-inequality prune instead of the occluding one).
+    "cosn768": dict(n=1_000_000, dim=768, normalized=True, metric=3, comps=0, sigma=0.0,
+                    nq=10_000, R=64, l_build=128, alpha=1.2, pq_chunks=0, pq_train=0, k=10,
+                    l_sweep=[128, 192, 256], strategies=["fp32", "bf16", "fp8"],
+                    seed=0xD15CA77 + 3),
+    # The served-stream shape: 10M x 96 mixture of 1,024 components, R = 48.
+    "mix10m": dict(n=10_000_000, dim=96, comps=1024, sigma=8.0, nq=10_000, R=48, l_build=100,
+                   alpha=1.2, pq_chunks=0, pq_train=0, k=10, l_sweep=[64, 128, 256, 512],
+                   strategies=["fp32", "bf16", "fp8"], seed=0xD15CA77 + 4),
 }
 TARGET_RECALL = 0.95
 METRIC_NAME = "QPS at recall@10>=0.95"
+
+
+def metric_of(w: dict):
+    from diskann_b200 import Metric
+
+    return Metric(w.get("metric", 2))
 
 
 def log(*a):
@@ -78,16 +100,21 @@ def prepare(name: str, rank: int, cache_root: str):
     elif not os.path.exists(ready):
         os.makedirs(cdir, exist_ok=True)
         t0 = time.time()
-        base, queries = datasets.gaussian_mixture(w["n"], w["dim"], w["comps"], w["sigma"],
-                                                  seed=w["seed"], n_queries=w["nq"])
+        if w.get("normalized"):
+            base, queries = datasets.normalized_gaussian(w["n"], w["dim"], w["seed"],
+                                                         n_queries=w["nq"])
+        else:
+            base, queries = datasets.gaussian_mixture(w["n"], w["dim"], w["comps"], w["sigma"],
+                                                      seed=w["seed"], n_queries=w["nq"])
         log(f"[prepare] data {time.time() - t0:.1f}s")
         t0 = time.time()
         import torch
 
         # Larger batches search on the GPU when there is one: the same graph as the host build.
         dev = 0 if torch.cuda.is_available() else None
-        vectors, adj, deg, n = graph.build_vamana(base, pruned_degree=w["R"], l_build=w["l_build"],
-                                                  alpha=w["alpha"], device=dev)
+        vectors, adj, deg, n = graph.build_vamana(base, metric=metric_of(w), pruned_degree=w["R"],
+                                                  l_build=w["l_build"], alpha=w["alpha"],
+                                                  device=dev)
         log(f"[prepare] vamana build ({'GPU searches' if dev is not None else 'host'}) "
             f"{time.time() - t0:.1f}s, mean degree {deg[:n].mean():.1f}")
         np.save(os.path.join(cdir, "vectors.npy"), vectors)
@@ -102,7 +129,7 @@ def prepare(name: str, rank: int, cache_root: str):
             np.save(os.path.join(cdir, "pq_pivots.npy"), pq.pivots)
             np.save(os.path.join(cdir, "pq_codes.npy"), pq.codes)
         t0 = time.time()
-        gt, _ = knn_f64(base, queries, w["k"], 2)
+        gt, _ = knn_f64(base, queries, w["k"], int(metric_of(w)))
         log(f"[prepare] float64 ground truth {time.time() - t0:.1f}s")
         np.save(os.path.join(cdir, "gt.npy"), gt)
         with open(ready, "w") as f:
@@ -230,6 +257,33 @@ def algorithmic_bytes(stats, w, l, mean_degree, strategy):
     return float(per.sum() + extra)
 
 
+def max_rel_dist_error(ids, dists, data, metric):
+    """Largest relative error of the returned float32 distances against the same pairs'
+    distances in float64 (the precision forms rerank with exact FP32 rows, so this is the
+    FP32 rounding of the final distances)."""
+    import torch
+
+    from diskann_b200 import Metric
+
+    valid = ids != 0xFFFFFFFF
+    if not valid.any():
+        return None
+    q = torch.from_numpy(data["queries"]).cuda().double()
+    rows = torch.from_numpy(data["vectors"][np.where(valid, ids, 0).astype(np.int64)]).cuda().double()
+    if metric == Metric.L2:
+        d = ((rows - q[:, None, :]) ** 2).sum(-1)
+    elif metric == Metric.INNER_PRODUCT:
+        d = -(rows * q[:, None, :]).sum(-1)
+    elif metric == Metric.COSINE:
+        d = 1.0 - (rows * q[:, None, :]).sum(-1) / (rows.norm(dim=-1) * q.norm(dim=-1)[:, None])
+    else:
+        d = 1.0 - (rows * q[:, None, :]).sum(-1)
+    got = torch.from_numpy(dists.astype(np.float64)).cuda()
+    rel = (got - d).abs() / d.abs().clamp_min(1e-12)
+    rel = torch.where(torch.from_numpy(valid).cuda(), rel, torch.zeros_like(rel))
+    return float(rel.max())
+
+
 def stats_array(st):
     out = np.zeros(st.shape[0], dtype=[("cmps", np.uint32), ("hops", np.uint32),
                                        ("result_count", np.uint32), ("flags", np.uint32)])
@@ -295,7 +349,7 @@ def run_ours(args, data, rank, world):
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
     t0 = time.time()
-    provider = GpuProvider(data["vectors"], data["adj"], data["deg"], data["n"], Metric.L2,
+    provider = GpuProvider(data["vectors"], data["adj"], data["deg"], data["n"], metric_of(w),
                            pq=data["pq"], device=dev, low_precision=("bf16", "fp8"))
     idx = DiskANNIndex(provider)
     log(f"[ours] index upload {time.time() - t0:.1f}s, {provider.info()['device_bytes'] / 2**20:.0f} MiB")
@@ -339,6 +393,11 @@ def run_ours(args, data, rank, world):
             row = {"L": l, "recall": round(r, 4), "reached": r >= TARGET_RECALL}
             if r >= TARGET_RECALL:
                 break
+        search(Knn(k, row["L"]), strat)
+        torch.cuda.synchronize()
+        err = max_rel_dist_error(ids.cpu().numpy().view(np.uint32), dists.cpu().numpy(), data,
+                                 metric_of(w))
+        row["max_rel_dist_err_vs_f64"] = None if err is None else float(f"{err:.3g}")
         row["qps"] = round(timed(Knn(k, row["L"]), strat), 1)
         table[name] = row
         log(f"[ours] {name}: {row}")
@@ -373,14 +432,20 @@ def run_ours(args, data, rank, world):
     ms_per_step = elapsed_ms / args.steps
     value = world * nq / (ms_per_step / 1e3)
 
-    # End to end through the C ABI with host buffers (pinned host memory).
+    # End to end through the C ABI with host buffers (pinned host memory for the queries and
+    # the caller-owned result buffers).
+    from diskann_b200 import STATS_DTYPE
+
     hq = torch.from_numpy(queries).pin_memory().numpy()
+    pinned = lambda shape, dt: torch.empty(shape, dtype=dt).pin_memory().numpy()  # noqa: E731
+    hout = (pinned((nq, k), torch.int32).view(np.uint32), pinned((nq, k), torch.float32),
+            pinned((nq * 16,), torch.uint8).view(STATS_DTYPE))
     e2e_t = []
     for s in range(args.warmup + args.steps):
         flush.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        idx.search(params, strategy, hq)
+        idx.search(params, strategy, hq, out=hout)
         t1 = time.perf_counter()
         if s >= args.warmup:
             e2e_t.append(t1 - t0)
@@ -416,7 +481,7 @@ def run_ours(args, data, rank, world):
                          d2h_bytes_per_step=int(nq * k * 8 + nq * 16)),
                 roofline=dict(bound="hbm", achieved=round(achieved, 1), peak=peak, unit="GB/s",
                               frac=round(achieved / peak, 4),
-                              traffic=traffic_from_profile(head, nq),
+                              traffic=traffic_from_profile(args.workload, head, nq),
                               algorithmic_bytes_per_step=int(alg), peak_source=peak_src),
                 clocks=clocks.summary(),
                 stats=dict(cmps_mean=float(stats_np["cmps"].mean()),
@@ -425,10 +490,10 @@ def run_ours(args, data, rank, world):
                 gpu_launches=2 * args.steps)
 
 
-def traffic_from_profile(strategy, nq):
+def traffic_from_profile(workload, strategy, nq):
     """DRAM bytes (read + write) per launch of the headline kernel, from the committed ncu
-    summary of the same workload (scaled to `nq` queries), or None."""
-    p = os.path.join(ROOT, "profiles", "dram_traffic_pq1m.json")
+    summary of the same workload (scaled to `nq` queries), or None when there is none."""
+    p = os.path.join(ROOT, "profiles", f"dram_traffic_{workload}.json")
     try:
         with open(p) as f:
             rec = json.load(f)[strategy]
@@ -456,7 +521,8 @@ def oracle_index(data):
     from oracle import oracle as orc
 
     pq = data["pq"]
-    return orc.OracleIndex(data["vectors"], data["adj"], data["deg"], data["n"], orc.METRIC_L2,
+    return orc.OracleIndex(data["vectors"], data["adj"], data["deg"], data["n"],
+                           int(metric_of(data["w"])),
                            *(tuple() if pq is None else (pq.offsets, pq.pivots, pq.codes)))
 
 
@@ -501,7 +567,7 @@ def next_rows(data, threads, build=True):
     q = data["queries"]
     nq = q.shape[0]
     out = {}
-    prov = GpuProvider(data["vectors"], data["adj"], data["deg"], n, Metric.L2)
+    prov = GpuProvider(data["vectors"], data["adj"], data["deg"], n, metric_of(w))
     idx = DiskANNIndex(prov)
     o = oracle_index(data)
     sample = min(300, nq)
@@ -545,16 +611,19 @@ def next_rows(data, threads, build=True):
     tags[n:] = 255
     ext = np.arange(total, dtype=np.uint64)
     ext[n:] = np.uint64(0xFFFFFFFFFFFFFFFF)
-    for name, typed, code in (("inmem_u8", np.clip(np.rint(data["vectors"]), 0, 255).astype(np.uint8), 2),
-                              ("inmem_f16", data["vectors"].astype(np.float16), 1)):
-        ip = InmemProvider(typed, data["adj"], data["deg"], n, tags, ext, Metric.L2)
+    kinds = [("inmem_f16", data["vectors"].astype(np.float16), 1)]
+    if not w.get("normalized"):  # values in [0, 255]: the u8 layer holds them after rounding
+        kinds.insert(0, ("inmem_u8", np.clip(np.rint(data["vectors"]), 0, 255).astype(np.uint8), 2))
+    for name, typed, code in kinds:
+        ip = InmemProvider(typed, data["adj"], data["deg"], n, tags, ext, metric_of(w))
         qt = (np.clip(np.rint(q), 0, 255).astype(np.uint8) if code == 2 else q.astype(np.float16))
         res = {}
         t = _median_time(lambda: res.__setitem__("r", ip.search(Knn(k, 50), qt)))
         recall = float(np.mean([len(set(res["r"][0][i].tolist()) & set(data["gt"][i].tolist())) / k
                                 for i in range(nq)]))
         ip.close()
-        oi = orc.OracleIndex(typed.astype(np.float32), data["adj"], data["deg"], n, orc.METRIC_L2)
+        oi = orc.OracleIndex(typed.astype(np.float32), data["adj"], data["deg"], n,
+                             int(metric_of(w)))
         rows = inmem_rows(typed, tags)
         t0 = time.perf_counter()
         for i in range(sample):
@@ -657,7 +726,7 @@ def profile_case(args):
     data = prepare(args.workload, 0, args.cache)
     w = data["w"]
     torch.cuda.set_device(0)
-    prov = GpuProvider(data["vectors"], data["adj"], data["deg"], data["n"], Metric.L2,
+    prov = GpuProvider(data["vectors"], data["adj"], data["deg"], data["n"], metric_of(w),
                        pq=data["pq"], low_precision=("bf16", "fp8"))
     idx = DiskANNIndex(prov)
     q = torch.from_numpy(data["queries"]).cuda()

@@ -7,8 +7,8 @@
 //    hop's work is small (one adjacency row, a few to a few dozen candidates), so the kernel
 //    is bound by dependent memory latency; one warp per query keeps many queries in flight
 //    per SM and every phase is warp-synchronous (ballots, shuffles, __syncwarp).
-//  * k_search_cta — one CTA (128 threads) per query: more lanes per hop for wide rows
-//    (D >= 384) or wide beams.  Its bitmap variant is the spill pass (below).
+//  * k_search_cta — one CTA (128 threads) per query: more lanes per hop for wide beams.  Its
+//    bitmap variant is the spill pass (below).
 //
 // Query state:
 //   * the candidate queue (diskann/src/neighbor/queue.rs:68-519): sorted (distance, id) arrays

@@ -117,7 +117,7 @@ extern "C" int32_t dk_search_device_noalloc(dk_index* ix, int32_t strategy, cons
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ix->device);
 
   const char* kenv = getenv("DK_KERNEL");
-  bool warp = ix->dim < 384 && beam_width <= 4;
+  bool warp = beam_width <= 4;
   if (kenv && !strcmp(kenv, "warp")) warp = true;
   if (kenv && !strcmp(kenv, "cta")) warp = false;
 

@@ -353,19 +353,29 @@ class DiskANNIndex:
     def __init__(self, provider: GpuProvider):
         self.provider = provider
 
-    def search(self, params: Knn, strategy: _Strategy, queries):
+    def search(self, params: Knn, strategy: _Strategy, queries, out=None):
         """Search host queries (nq, D) float32; returns ``(ids, distances, stats)`` numpy arrays.
 
         Host buffers cross the C ABI (``dk_search``): queries are copied to the device and
-        results back inside the call.
+        results back inside the call.  ``out``: optional caller-owned ``(ids, dists, stats)``
+        arrays to write into (uint32 (nq, k), float32 (nq, k), STATS_DTYPE (nq,)), as the
+        reference's search writes into the caller's output buffer; pinned host memory makes
+        the copies faster.
         """
         q = np.ascontiguousarray(np.atleast_2d(queries), dtype=np.float32)
         if q.shape[1] != self.provider.dim:
             raise ANNError(Status.DIMENSION_MISMATCH, f"query dim {q.shape[1]} != {self.provider.dim}")
         nq, k = q.shape[0], params.k_value
-        ids = np.empty((nq, k), dtype=np.uint32)
-        dists = np.empty((nq, k), dtype=np.float32)
-        stats = np.zeros(nq, dtype=STATS_DTYPE)
+        if out is not None:
+            ids, dists, stats = out
+            if (ids.shape != (nq, k) or ids.dtype != np.uint32 or dists.shape != (nq, k)
+                    or dists.dtype != np.float32 or stats.shape != (nq,) or stats.dtype != STATS_DTYPE
+                    or not all(a.flags["C_CONTIGUOUS"] for a in out)):
+                raise ANNError(Status.INVALID_ARGUMENT, "out arrays do not match (nq, k)")
+        else:
+            ids = np.empty((nq, k), dtype=np.uint32)
+            dists = np.empty((nq, k), dtype=np.float32)
+            stats = np.zeros(nq, dtype=STATS_DTYPE)
         _check(_native.load().dk_search(
             self.provider.handle, strategy.code, q.ctypes.data, q.shape[1], nq, k,
             params.l_value, params.beam_width, ids.ctypes.data, dists.ctypes.data, stats.ctypes.data,

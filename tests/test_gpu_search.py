@@ -11,8 +11,8 @@ import os
 import numpy as np
 import pytest
 
-from diskann_b200 import (ANNError, DiskANNIndex, FullPrecision, GpuProvider, Hybrid, Knn,
-                          Metric, PQData, Quantized, Status, datasets)
+from diskann_b200 import (STATS_DTYPE, ANNError, DiskANNIndex, FullPrecision, GpuProvider,
+                          Hybrid, Knn, Metric, PQData, Quantized, Status, datasets)
 from oracle import oracle as O
 from tests.helpers import queries_like, random_index, simple_pq
 
@@ -185,6 +185,12 @@ def test_device_entry_point_matches_host_entry_point(nq):
     q = queries_like(v[:n], nq, seed=72)
     idx = DiskANNIndex(GpuProvider(v, a, d, n, Metric.L2))
     hi, hd, hs = idx.search(Knn(10, 50), FullPrecision(), q)
+    out = (np.empty((nq, 10), np.uint32), np.empty((nq, 10), np.float32), np.empty(nq, STATS_DTYPE))
+    oi, od, os_ = idx.search(Knn(10, 50), FullPrecision(), q, out=out)
+    assert oi is out[0]
+    np.testing.assert_array_equal(oi, hi)
+    np.testing.assert_array_equal(od, hd)
+    np.testing.assert_array_equal(os_, hs)
     dq = torch.from_numpy(q).cuda()
     ids = torch.empty((nq, 10), dtype=torch.int32, device="cuda")
     dists = torch.empty((nq, 10), dtype=torch.float32, device="cuda")
