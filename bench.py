@@ -722,6 +722,16 @@ def profile_case(args):
         torch.cuda.set_device(0)
         log(f"[profile] next rows {next_rows(data, os.cpu_count() or 1, build=False)}")
         return 0
+    if args.profile == "build":  # graph construction of a 100k-point prefix on the GPU
+        from diskann_b200 import graph
+
+        data = prepare(args.workload, 0, args.cache)
+        w = data["w"]
+        t0 = time.perf_counter()
+        graph.build_vamana(data["vectors"][: min(100_000, data["n"])], metric=metric_of(w),
+                           pruned_degree=w["R"], l_build=w["l_build"], alpha=w["alpha"], device=0)
+        log(f"[profile] build {time.perf_counter() - t0:.2f}s")
+        return 0
     name, l = args.profile.split(":")
     data = prepare(args.workload, 0, args.cache)
     w = data["w"]
@@ -757,7 +767,8 @@ def main():
     ap.add_argument("--profile", default=None, metavar="STRATEGY:L",
                     help="profiling case for ncu: upload the workload's index and run two "
                          "batched searches (warm-up, profiled), no timing, no JSON line; "
-                         "'next' runs the range / paged / inmem measurements instead")
+                         "'next' runs the range / paged / inmem measurements instead, 'build' "
+                         "the construction of a 100k-point prefix")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
