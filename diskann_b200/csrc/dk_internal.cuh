@@ -113,6 +113,8 @@ struct SearchParams {
   const unsigned char* raw;
   uint32_t raw_stride;
   const uint32_t* readable;
+  // FullPrecision output without FilterStartPoints (range search's first round).
+  uint32_t keep_start;
 };
 
 constexpr uint32_t kFlagSpilled = 1u;
@@ -179,8 +181,10 @@ struct SearchRecord {
 };
 
 // Launch the search (first pass + spill pass) on `stream`.  Parameters are validated by
-// the caller.
+// the caller.  `keep_start`: the FullPrecision output keeps start points (range search's
+// first round reads the queue as it stands).
 int32_t dk_launch_search(dk_index* ix, int32_t strategy, const float* queries,
                          uint64_t qstride, uint32_t nq, uint32_t k, uint32_t l, uint32_t beam,
                          uint32_t* ids, float* dists, dk_search_stats* stats,
-                         cudaStream_t stream, const SearchRecord* record = nullptr);
+                         cudaStream_t stream, const SearchRecord* record = nullptr,
+                         bool keep_start = false);

@@ -1090,7 +1090,7 @@ __device__ void cta_post_process(const SearchParams& P, const State& S, uint32_t
   for (uint32_t t0 = 0; t0 < size; t0 += NT) {
     const uint32_t i = t0 + tid;
     const uint32_t id = i < size ? (qi[i] & kIdMask) : 0u;
-    const bool keep = i < size && id < P.n;  // FilterStartPoints (glue.rs:730-773)
+    const bool keep = i < size && (id < P.n || P.keep_start);  // FilterStartPoints (glue.rs:730-773)
     uint32_t total;
     const uint32_t pos = base + block_scan<NT>(keep, M->warp_sums, total);
     if (keep) {
@@ -1501,7 +1501,7 @@ __device__ void warp_post_process(const SearchParams& P, const State& S, const Q
     if (!hybrid && base >= k) break;
     const uint32_t i = t0 + lane;
     const uint32_t id = i < size ? (qi[i] & kIdMask) : 0u;
-    const bool keep = i < size && id < P.n;  // FilterStartPoints (glue.rs:730-773)
+    const bool keep = i < size && (id < P.n || P.keep_start);  // FilterStartPoints (glue.rs:730-773)
     const uint32_t m = __ballot_sync(kFull, keep);
     const uint32_t pos = base + __popc(m & lanemask_lt());
     if (keep) {

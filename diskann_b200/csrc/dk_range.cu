@@ -1,17 +1,19 @@
 // Range search (the reference's `Range`, diskann/src/graph/search/range_search.rs) with the
-// FullPrecision accessor, one 128-thread CTA per query, persistent over the batch.
+// FullPrecision accessor, in two launches per batch.
 //
-// Per query: the first round is the batch path's CTA search (cta_search) with a queue of
-// starting_l + F entries and an exact per-CTA bitmap as the visited set; in_range is the first
-// starting_l queue entries with distance <= radius (range_search.rs:179-193); the bitmap is
-// cleared and refilled with them; when |in_range| >= (starting_l as f32 * initial_slack) and
-// |in_range| < max_returned the second round (range_search_internal, range_search.rs:331-389)
-// walks a FIFO frontier - which is in_range itself, in order - popping beam_width nodes,
-// expanding them through the visited set and appending every scored neighbour with distance
-// <= radius * range_slack while |in_range| < max_returned; the post-processor drops start
-// points and keeps inner_radius < distance <= radius, in order.  Stats follow the reference:
-// cmps of the first round; with a second round, hops = first-round hops + (first-round hops
-// + second-round hops) (the scratch counter carries the first round's hops).
+// Round one is the k-NN search itself (dk_launch_search, the warp-per-query kernel) with
+// L = k = starting_l and the start points kept in its output: the queue's first starting_l
+// entries, in order, which is what range_search.rs:179-193 reads.  k_range_rest then, one
+// 128-thread CTA per query (persistent, each CTA owning an exact bitmap): in_range is those
+// entries with distance <= radius, written straight into the caller's output row; when
+// |in_range| >= (starting_l as f32 * initial_slack) and |in_range| < max_returned, the second
+// round (range_search_internal, range_search.rs:331-389) starts from a visited set holding
+// exactly in_range and walks a FIFO frontier - in_range itself, in order - popping beam_width
+// nodes, expanding them through the visited set and appending every scored neighbour with
+// distance <= radius * range_slack while |in_range| < max_returned.  The post-processor drops
+// start points and keeps inner_radius < distance <= radius, in order.  Stats follow the
+// reference: cmps of the first round; with a second round, hops = first-round hops +
+// (first-round hops + second-round hops) (the scratch counter carries the first round's hops).
 //
 // in_range lives in the caller's output rows (capacity entries per query) and is compacted in
 // place at the end.  With max_returned unlimited the capacity bounds it instead; a query that
@@ -38,10 +40,14 @@ struct RangeParams {
   uint32_t starting_l;
   uint32_t max_returned;  // 0: unlimited (bounded by capacity)
   uint32_t capacity;      // output entries per query
+  // Round one's output: starting_l entries per query, and its stats.
+  const uint32_t* first_ids;
+  const float* first_d;
+  const dk_search_stats* first_stats;
 };
 
 template <int NT, int METRIC, int DIM>
-__global__ void __launch_bounds__(NT) k_range_cta(const SearchParams P, const RangeParams R) {
+__global__ void __launch_bounds__(NT) k_range_rest(const SearchParams P, const RangeParams R) {
   extern __shared__ __align__(16) unsigned char smem[];
   const State S = carve(smem, P);
   const uint32_t tid = threadIdx.x;
@@ -49,37 +55,38 @@ __global__ void __launch_bounds__(NT) k_range_cta(const SearchParams P, const Ra
   BitmapSet vset{P.bitmap + (size_t)blockIdx.x * P.bitmap_words, P.bitmap_words};
   const uint32_t max_ret = R.max_returned ? R.max_returned : R.capacity;
   const float limit = R.radius * R.range_slack;
+  const uint32_t dpad = (P.dim + 15u) & ~15u;
   for (uint32_t qid = blockIdx.x; qid < P.nq; qid += gridDim.x) {
     uint32_t* out_ids = P.out_ids + (size_t)qid * R.capacity;
     float* out_d = P.out_dists + (size_t)qid * R.capacity;
-    __syncthreads();
-    uint32_t cmps = 0, hops = 0;
-    cta_search<NT, METRIC, kModeFP32, DIM>(P, S, vset, qid, cmps, hops);
+    const uint32_t* fi = R.first_ids + (size_t)qid * R.starting_l;
+    const float* fd = R.first_d + (size_t)qid * R.starting_l;
+    const dk_search_stats first = R.first_stats[qid];
     __syncthreads();
     // in_range: the first starting_l queue entries within the radius, in queue order.
-    const float* qd = S.qd[M->cur];
-    const uint32_t* qi = S.qi[M->cur];
-    const uint32_t n_iter = min(M->size, R.starting_l);
+    const uint32_t n_iter = min(first.result_count, R.starting_l);
     uint32_t n_in = 0;
     for (uint32_t i0 = 0; i0 < n_iter; i0 += NT) {
       const uint32_t i = i0 + tid;
-      const bool in = i < n_iter && qd[i] <= R.radius;
+      const bool in = i < n_iter && fd[i] <= R.radius;
       uint32_t total;
       const uint32_t pos = block_scan<NT>(in, M->warp_sums, total);
       if (in && n_in + pos < max_ret) {
-        out_ids[n_in + pos] = qi[i] & kIdMask;
-        out_d[n_in + pos] = qd[i];
+        out_ids[n_in + pos] = fi[i];
+        out_d[n_in + pos] = fd[i];
       }
       n_in = min(n_in + total, max_ret);
     }
     __syncthreads();
-    vset.clear(tid, NT);
-    __syncthreads();
-    for (uint32_t i = tid; i < n_in; i += NT) vset.insert(out_ids[i]);
-    __syncthreads();
     const bool second = n_in >= (uint32_t)((float)R.starting_l * R.initial_slack) && n_in < max_ret;
     uint32_t range_hops = 0;
     if (second) {
+      const float* qsrc = P.queries + (size_t)qid * P.qstride;
+      for (uint32_t i = tid; i < dpad; i += NT) S.q[i] = i < P.dim ? qsrc[i] : 0.0f;
+      vset.clear(tid, NT);
+      __syncthreads();
+      for (uint32_t i = tid; i < n_in; i += NT) vset.insert(out_ids[i]);
+      __syncthreads();
       uint32_t front = 0;
       while (front < n_in && n_in < max_ret) {
         const uint32_t nb = min(P.beam, n_in - front);
@@ -149,8 +156,8 @@ __global__ void __launch_bounds__(NT) k_range_cta(const SearchParams P, const Ra
     }
     if (tid == 0) {
       const bool truncated = R.max_returned == 0 && n_in >= R.capacity;
-      P.stats[qid] = dk_search_stats{cmps, second ? hops + hops + range_hops : hops, written,
-                                     (second ? 2u : 0u) | (truncated ? 4u : 0u)};
+      P.stats[qid] = dk_search_stats{first.cmps, second ? first.hops + first.hops + range_hops : first.hops,
+                                     written, (second ? 2u : 0u) | (truncated ? 4u : 0u)};
     }
   }
 }
@@ -159,7 +166,7 @@ __global__ void __launch_bounds__(NT) k_range_cta(const SearchParams P, const Ra
 template <int METRIC, int DIM>
 cudaError_t launch_range(const SearchParams& P, const RangeParams& R, uint32_t grid,
                          cudaStream_t stream, int* occupancy) {
-  auto k = k_range_cta<kCtaThreads, METRIC, DIM>;
+  auto k = k_range_rest<kCtaThreads, METRIC, DIM>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P.smem_bytes);
   if (e != cudaSuccess) return e;
   if (occupancy)
@@ -220,11 +227,14 @@ int32_t check_range(const dk_index* ix, uint32_t starting_l, uint32_t beam_width
 }
 
 int32_t launch_range_search(dk_index* ix, const float* queries, uint64_t qstride, uint32_t nq,
-                            const RangeParams& R, uint32_t beam, uint32_t* ids, float* dists,
+                            const RangeParams& R0, uint32_t beam, uint32_t* ids, float* dists,
                             dk_search_stats* stats, cudaStream_t stream) {
   if (nq == 0) return DK_OK;
+  RangeParams R = R0;
+  const uint32_t sl = R.starting_l;
   SearchParams P{};
-  dk::base_params(ix, DK_STRATEGY_FULL_PRECISION, 1, R.starting_l, beam, P);
+  dk::base_params(ix, DK_STRATEGY_FULL_PRECISION, 1, sl, beam, P);
+  P.cap = 0;  // round two keeps no queue; its lists hold beam x max_degree candidates
   P.queries = queries;
   P.qstride = qstride;
   P.nq = nq;
@@ -237,8 +247,8 @@ int32_t launch_range_search(dk_index* ix, const float* queries, uint64_t qstride
   cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ix->device);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ix->device);
   if (P.smem_bytes > (uint32_t)max_optin)
-    return fail(DK_ERR_UNSUPPORTED, "search state does not fit in shared memory (starting_l too large)");
-  // One exact bitmap over all ids per resident CTA (occupancy), within 512 MiB.
+    return fail(DK_ERR_UNSUPPORTED, "search state does not fit in shared memory");
+  // Round two: one exact bitmap over all ids per resident CTA (occupancy), within 512 MiB.
   const uint32_t words = (ix->n + ix->f + 31u) / 32u;
   const uint64_t per = (uint64_t)words * 4u;
   int occ = 0;
@@ -246,14 +256,32 @@ int32_t launch_range_search(dk_index* ix, const float* queries, uint64_t qstride
   if (eo != cudaSuccess) return fail(DK_ERR_CUDA, std::string("range occupancy: ") + cudaGetErrorString(eo));
   uint32_t grid = std::min<uint32_t>(nq, (uint32_t)std::max(1, occ) * (uint32_t)std::max(1, sms));
   if (per * grid > (512ull << 20)) grid = (uint32_t)std::max<uint64_t>(1, (512ull << 20) / per);
+  // Scratch: round one's ids | distances | stats | round two's bitmaps.
+  auto up = [](uint64_t x) { return (x + 255) / 256 * 256; };
+  const uint64_t o_d = up((uint64_t)nq * sl * 4), o_st = o_d + up((uint64_t)nq * sl * 4);
+  const uint64_t o_bm = o_st + up((uint64_t)nq * sizeof(dk_search_stats));
   unsigned char* scratch = nullptr;
-  cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&scratch), per * grid, ix->pool, stream);
+  cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&scratch), o_bm + per * grid,
+                                          ix->pool, stream);
   if (e != cudaSuccess)
     return fail(DK_ERR_OUT_OF_MEMORY, std::string("range scratch: ") + cudaGetErrorString(e));
-  P.bitmap = reinterpret_cast<uint32_t*>(scratch);
-  P.bitmap_words = words;
-  e = range_dispatch(ix->metric, P, R, grid, stream, nullptr);
+  uint32_t* first_ids = reinterpret_cast<uint32_t*>(scratch);
+  float* first_d = reinterpret_cast<float*>(scratch + o_d);
+  dk_search_stats* first_st = reinterpret_cast<dk_search_stats*>(scratch + o_st);
+  // Round one: the k-NN search with L = k = starting_l, start points kept in its output.
+  const int32_t rc = dk_launch_search(ix, DK_STRATEGY_FULL_PRECISION, queries, qstride, nq, sl,
+                                      sl, beam, first_ids, first_d, first_st, stream, nullptr,
+                                      true);
+  if (rc == DK_OK) {
+    R.first_ids = first_ids;
+    R.first_d = first_d;
+    R.first_stats = first_st;
+    P.bitmap = reinterpret_cast<uint32_t*>(scratch + o_bm);
+    P.bitmap_words = words;
+    e = range_dispatch(ix->metric, P, R, grid, stream, nullptr);
+  }
   cudaFreeAsync(scratch, stream);
+  if (rc != DK_OK) return rc;
   if (e != cudaSuccess) return fail(DK_ERR_CUDA, std::string("range launch: ") + cudaGetErrorString(e));
   return DK_OK;
 }

@@ -189,7 +189,7 @@ int32_t plan_warp(dk_index* ix, SearchParams& P, LaunchPlan& L, int mode, double
 int32_t dk_launch_search(dk_index* ix, int32_t strategy, const float* queries,
                          uint64_t qstride, uint32_t nq, uint32_t k, uint32_t l, uint32_t beam,
                          uint32_t* ids, float* dists, dk_search_stats* stats,
-                         cudaStream_t stream, const SearchRecord* record) {
+                         cudaStream_t stream, const SearchRecord* record, bool keep_start) {
   if (nq == 0) return DK_OK;
   const int mode = mode_of_strategy(strategy);
   const bool pq = mode == kModePQ;
@@ -202,6 +202,7 @@ int32_t dk_launch_search(dk_index* ix, int32_t strategy, const float* queries,
   P.out_dists = dists;
   P.stats = stats;
   P.hint = ix->hint_dev;
+  P.keep_start = keep_start ? 1u : 0u;
   if (record) {
     P.rec_ids = record->ids;
     P.rec_d = record->dists;
