@@ -425,7 +425,9 @@ def run_ours(args, data, rank, world):
             ev[s][1].record(stream)
         torch.cuda.synchronize()
     barrier(world)
-    elapsed_ms = sum(a.elapsed_time(b) for a, b in ev)
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    log(f"[ours] timed steps (ms): {[round(x, 3) for x in step_ms]}")
+    elapsed_ms = sum(step_ms)
     elapsed_ms = max_over_ranks(elapsed_ms, world)
     stats_np = stats_array(stats.cpu().numpy().view(np.uint32))
     rec = recall_at_k(ids.cpu().numpy().view(np.uint32), gt, k)
