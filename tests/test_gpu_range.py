@@ -67,7 +67,7 @@ def test_range_parity_with_the_oracle(metric, dim):
     inner = float(d0[0, 2])
     for p in [Range(40, r), Range(40, r, inner_radius=inner), Range(40, r, beam_width=2),
               Range(40, r, range_slack=1.3, initial_slack=0.5), Range(40, r, max_returned=60),
-              Range(8, r * 1.5, max_returned=120)]:
+              Range(8, r * 1.5, max_returned=120), Range(40, r, beam_width=8)]:
         _assert_same(idx, orc, q, p, capacity=p.max_returned or 4000)
 
 
@@ -83,3 +83,41 @@ def test_range_errors():
     with pytest.raises(ANNError) as e:
         idx.range_search(Range(10, 1.0), v[:2, :8])
     assert e.value.status == Status.DIMENSION_MISMATCH
+
+
+def test_range_device_entry_point_matches_host_entry_point():
+    """dk_range_search_device (device buffers, caller's stream) returns what dk_range_search
+    returns."""
+    import ctypes
+
+    import torch
+
+    from diskann_b200 import STATS_DTYPE, _native
+
+    v, a, d, n = random_index(3000, 64, 24, seed=77, max_degree=31)
+    q = queries_like(v[:n], 40, seed=8)
+    idx = DiskANNIndex(GpuProvider(v, a, d, n, Metric.L2))
+    orc = O.OracleIndex(v, a, d, n, O.METRIC_L2)
+    _, d0, _ = orc.search(q[:1], 40, 80, 1)
+    p = Range(40, float(d0[0, 20]), max_returned=200)
+    host, hst = idx.range_search(p, q, capacity=200)
+    dq = torch.from_numpy(q).cuda()
+    ids = torch.empty((40, 200), dtype=torch.int32, device="cuda")
+    dists = torch.empty((40, 200), dtype=torch.float32, device="cuda")
+    st = torch.empty((40, 4), dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream()
+    rc = _native.load().dk_range_search_device(
+        idx.provider.handle, dq.data_ptr(), 64, 40, p.starting_l, p.beam_width, p.radius,
+        float("nan"), p.initial_slack, p.range_slack, p.max_returned, 200, ids.data_ptr(),
+        dists.data_ptr(), st.data_ptr(), ctypes.c_void_p(stream.cuda_stream))
+    assert rc == 0
+    torch.cuda.synchronize()
+    ids_h = ids.cpu().numpy().view(np.uint32)
+    d_h = dists.cpu().numpy()
+    st_h = st.cpu().numpy().view(np.uint32).reshape(-1).view(STATS_DTYPE)
+    for i in range(40):
+        c = int(st_h[i]["result_count"])
+        assert c == int(hst[i]["result_count"])
+        np.testing.assert_array_equal(ids_h[i, :c], host[i][0])
+        np.testing.assert_array_equal(d_h[i, :c].view(np.uint32), host[i][1].view(np.uint32))
+        assert int(st_h[i]["cmps"]) == int(hst[i]["cmps"])
