@@ -115,6 +115,11 @@ struct SearchParams {
   const uint32_t* readable;
   // FullPrecision output without FilterStartPoints (range search's first round).
   uint32_t keep_start;
+  // Serving: after a query's results are written, done_flags[qid] = done_value (mapped host
+  // memory, written after a system-scope fence), so the host can collect each request on its
+  // own; null elsewhere.
+  uint32_t* done_flags;
+  uint32_t done_value;
 };
 
 constexpr uint32_t kFlagSpilled = 1u;

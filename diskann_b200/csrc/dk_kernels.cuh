@@ -1726,6 +1726,14 @@ __global__ void __launch_bounds__(128, (MODE == kModeBF16 || MODE == kModeFP8) ?
                      P.rec_ids ? P.rec_ids + (size_t)qid * P.rec_cap : nullptr,
                      P.rec_ids ? P.rec_d + (size_t)qid * P.rec_cap : nullptr};
     warp_query<METRIC, MODE, DIM, U>(P, S, vset, io, lane);
+    if (P.done_flags) {  // serving: publish this request (results first, then its flag)
+      __threadfence_system();
+      __syncwarp();
+      if (lane == 0) {
+        __threadfence_system();
+        *reinterpret_cast<volatile uint32_t*>(P.done_flags + qid) = P.done_value;
+      }
+    }
     __syncwarp();
     gdirty = vset.gcount != 0u;
   }

@@ -5,6 +5,9 @@
 // k/L, results, a work counter and one global visited table per warp) and pinned staging.
 // Requests queue on submit and go out as soon as a context is free: one launch carries every
 // request queued at that moment, and launches on different contexts overlap on the device.
+// Each request completes on its own: the kernel writes its results straight into the
+// context's mapped pinned memory and then, after a system-scope fence, the request's done
+// flag, which the host polls; a short request does not wait for a long one in its launch.
 // The kernel is the batch path's warp-per-query kernel reading each request's own k and L,
 // so a request's results do not depend on what else is in flight.  No device code waits on
 // the host: a launch is an ordinary finite kernel, and the host learns of its end through
@@ -16,6 +19,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstdint>
 #include <cstring>
@@ -34,13 +38,16 @@ enum : uint8_t { kFree = 0, kPending = 1, kInFlight = 2, kDone = 3 };
 
 // One launch context.  Device buffer layout (each part 256-B aligned):
 // counter | kl[cap][2] | queries[cap][dim] | ids[cap][max_k] | dists[cap][max_k] |
-// stats[cap] | visited tables[slots][table].  Pinned staging mirrors kl .. stats.
+// stats[cap] | visited tables[slots][table].  Mapped pinned memory mirrors kl .. stats (the
+// kernel writes results there) and holds the per-request done flags after them.
 struct Context {
   cudaStream_t stream = nullptr;
   cudaEvent_t done = nullptr;
   unsigned char* dev = nullptr;
   unsigned char* host = nullptr;
+  unsigned char* host_dev = nullptr;  // the device's pointer to `host`
   std::vector<uint64_t> tickets;
+  uint32_t seq = 0;  // this context's launch count: the done-flag value of its current launch
   bool busy = false;
 };
 
@@ -55,6 +62,7 @@ struct dk_server {
   std::vector<Context> ctx;
   // Offsets inside a context's buffers.
   uint64_t off_kl = 0, off_q = 0, off_ids = 0, off_d = 0, off_st = 0, off_gt = 0, dev_bytes = 0;
+  uint64_t off_flag = 0;  // host buffers: done flags
   uint64_t host_bytes = 0;
   // Outstanding requests, indexed by ticket % queue_depth.
   std::vector<uint8_t> state;
@@ -100,27 +108,34 @@ void release(dk_server* s) {
   delete s;
 }
 
-// Collect the results of finished launches into the request table.
+// Collect finished requests into the request table: each request as soon as its done flag
+// is up, and a context's remaining ones when its launch has ended.
 int32_t reap(dk_server* s) {
   const uint32_t max_k = s->cfg.max_k, depth = s->cfg.queue_depth;
   for (Context& c : s->ctx) {
     if (!c.busy) continue;
     const cudaError_t q = cudaEventQuery(c.done);
-    if (q == cudaErrorNotReady) continue;
-    if (q != cudaSuccess) return cuda_fail(q, "serving launch");
+    if (q != cudaErrorNotReady && q != cudaSuccess) return cuda_fail(q, "serving launch");
+    const bool ended = q == cudaSuccess;
+    const volatile uint32_t* flag = reinterpret_cast<const volatile uint32_t*>(c.host + s->off_flag);
     const uint32_t* ids = reinterpret_cast<const uint32_t*>(c.host + s->off_ids);
     const float* d = reinterpret_cast<const float*>(c.host + s->off_d);
     const dk_search_stats* st = reinterpret_cast<const dk_search_stats*>(c.host + s->off_st);
     for (size_t i = 0; i < c.tickets.size(); ++i) {
       const uint32_t r = (uint32_t)(c.tickets[i] % depth);
+      if (s->state[r] != kInFlight) continue;
+      if (!ended && flag[i] != c.seq) continue;
+      std::atomic_thread_fence(std::memory_order_acquire);
       const uint32_t k = s->req_k[r];
       memcpy(&s->res_ids[(size_t)r * max_k], ids + i * max_k, 4ull * k);
       memcpy(&s->res_dists[(size_t)r * max_k], d + i * max_k, 4ull * k);
       s->res_stats[r] = st[i];
       s->state[r] = kDone;
     }
-    c.tickets.clear();
-    c.busy = false;
+    if (ended) {
+      c.tickets.clear();
+      c.busy = false;
+    }
   }
   return DK_OK;
 }
@@ -151,9 +166,13 @@ int32_t launch_pending(dk_server* s) {
     L.p1.req_kl = reinterpret_cast<const uint32_t*>(c.dev + s->off_kl);
     L.p1.queries = reinterpret_cast<const float*>(c.dev + s->off_q);
     L.p1.qstride = dim;
-    L.p1.out_ids = reinterpret_cast<uint32_t*>(c.dev + s->off_ids);
-    L.p1.out_dists = reinterpret_cast<float*>(c.dev + s->off_d);
-    L.p1.stats = reinterpret_cast<dk_search_stats*>(c.dev + s->off_st);
+    ++c.seq;
+    if (c.seq == 0) c.seq = 1;  // flags start at 0: never a launch's value
+    L.p1.out_ids = reinterpret_cast<uint32_t*>(c.host_dev + s->off_ids);
+    L.p1.out_dists = reinterpret_cast<float*>(c.host_dev + s->off_d);
+    L.p1.stats = reinterpret_cast<dk_search_stats*>(c.host_dev + s->off_st);
+    L.p1.done_flags = reinterpret_cast<uint32_t*>(c.host_dev + s->off_flag);
+    L.p1.done_value = c.seq;
     L.p1.work_counter = reinterpret_cast<uint32_t*>(c.dev);
     L.p1.gtable = reinterpret_cast<uint32_t*>(c.dev + s->off_gt);
     L.grid = std::min<uint32_t>(L.grid, (b + L.warps_per_cta - 1) / L.warps_per_cta);
@@ -162,15 +181,6 @@ int32_t launch_pending(dk_server* s) {
       e = cudaMemcpyAsync(c.dev + s->off_q, q, 4ull * dim * b, cudaMemcpyHostToDevice, c.stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(c.dev, 0, 4, c.stream);
     if (e == cudaSuccess) e = dk::dispatch(s->ix->metric, L, s->mode, c.stream);
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(c.host + s->off_ids, c.dev + s->off_ids, 4ull * max_k * b,
-                          cudaMemcpyDeviceToHost, c.stream);
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(c.host + s->off_d, c.dev + s->off_d, 4ull * max_k * b,
-                          cudaMemcpyDeviceToHost, c.stream);
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(c.host + s->off_st, c.dev + s->off_st, sizeof(dk_search_stats) * b,
-                          cudaMemcpyDeviceToHost, c.stream);
     if (e == cudaSuccess) e = cudaEventRecord(c.done, c.stream);
     if (e != cudaSuccess) return cuda_fail(e, "serving launch");
     c.busy = true;
@@ -229,7 +239,8 @@ extern "C" int32_t dk_server_create(dk_index* ix, const dk_server_config* cfg, d
   s->off_d = round_up(s->off_ids + 4ull * max_k * depth, 256);
   s->off_st = round_up(s->off_d + 4ull * max_k * depth, 256);
   s->off_gt = round_up(s->off_st + sizeof(dk_search_stats) * depth, 256);
-  s->host_bytes = s->off_gt;
+  s->off_flag = s->off_gt;
+  s->host_bytes = round_up(s->off_flag + 4ull * depth, 256);
   const uint64_t table_bytes = 4ull << P.gtable_log2;
   const uint64_t per_cta_tables = table_bytes * s->plan.warps_per_cta;
   size_t free_b = 0, total_b = 0;
@@ -253,7 +264,10 @@ extern "C" int32_t dk_server_create(dk_index* ix, const dk_server_config* cfg, d
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&c.dev), s->dev_bytes);
-    if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void**>(&c.host), s->host_bytes, 0);
+    if (e == cudaSuccess)
+      e = cudaHostAlloc(reinterpret_cast<void**>(&c.host), s->host_bytes, cudaHostAllocMapped);
+    if (e == cudaSuccess) e = cudaHostGetDevicePointer(reinterpret_cast<void**>(&c.host_dev), c.host, 0);
+    if (e == cudaSuccess) memset(c.host, 0, s->host_bytes);
   }
   const uint64_t rerun_bytes = round_up(4ull * dim, 256) + 2 * round_up(4ull * max_k, 256) +
                                sizeof(dk_search_stats);
