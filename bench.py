@@ -292,7 +292,8 @@ def stats_array(st):
     return out
 
 
-def serve_latency(provider, strategy, queries, gt, k, l, rate, seconds, mixed=False, seed=1):
+def serve_latency(provider, strategy, queries, gt, k, l, rate, seconds, mixed=False, seed=1,
+                  streams=0):
     """Poisson arrivals at `rate` requests/s replayed natively through the serving API
     (dk_server_replay from one host thread); latency = completion seen by the host - scheduled
     arrival.  `mixed`: each request draws k from {10, 50, 100} and L from {64, 128, 256, 512}
@@ -310,7 +311,7 @@ def serve_latency(provider, strategy, queries, gt, k, l, rate, seconds, mixed=Fa
         ks = np.full(n, k)
         ls = np.full(n, l)
     srv = SearchServer(provider, strategy, max_k=int(ks.max()), max_l=int(ls.max()),
-                       queue_depth=16384)
+                       queue_depth=16384, streams=streams)
     srv.replay(queries[:64], ks[:64], ls[:64], np.zeros(64))  # warm-up
     t0 = time.perf_counter()
     lat, ids, _ = srv.replay(queries, ks, ls, arrivals, want_results=True)

@@ -212,7 +212,7 @@ extern "C" int32_t dk_server_create(dk_index* ix, const dk_server_config* cfg, d
   dk_server* s = new dk_server();
   s->ix = ix;
   s->cfg = *cfg;
-  if (s->cfg.streams == 0) s->cfg.streams = 4;
+  if (s->cfg.streams == 0) s->cfg.streams = 16;
   s->mode = mode_of_strategy(cfg->strategy);
   const uint32_t dim = ix->dim, max_k = cfg->max_k, depth = cfg->queue_depth;
 

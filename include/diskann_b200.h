@@ -296,7 +296,7 @@ typedef struct dk_server_config {
   uint32_t beam_width;   /* for every request (<= 4) */
   uint32_t queue_depth;  /* outstanding requests accepted */
   uint32_t max_slots;    /* concurrent searches per launch (0 = all resident warps) */
-  uint32_t streams;      /* launch contexts that overlap on the device (0 = 4) */
+  uint32_t streams;      /* launch contexts that overlap on the device (0 = 16) */
 } dk_server_config;
 
 typedef struct dk_server_info {
