@@ -1690,12 +1690,13 @@ __device__ __forceinline__ void warp_query(const SearchParams& P, const State& S
 // Persistent grid: every warp owns a shared-memory slice and a global overflow table and
 // takes queries from a work counter until the batch is done.
 template <int METRIC, int MODE, int DIM, int U>
-// FP32 / PQ: the explicit minimum of one resident block lets the compiler give each thread up
-// to 255 registers; it takes ~170 here, and the kernel measured ~1.6x faster that way than with
-// the compiler's own choice for `__launch_bounds__(128)` alone (96 registers and spills).
-// BF16 / FP8: a minimum of four blocks caps them at 128 registers (121-127 used, no spills),
-// measured 5-9% faster on a 1M-point graph than with ~160 registers.
-__global__ void __launch_bounds__(128, (MODE == kModeBF16 || MODE == kModeFP8) ? 4 : 1)
+// Register budget.  The compiler's own choice for `__launch_bounds__(128)` alone is 96
+// registers with heavy spills (~1.6x slower).  FP32 / BF16 / FP8: a minimum of four resident
+// blocks caps them at 128 registers (FP32 at D = 128 with four rows per subgroup spills 12
+// bytes; no other variant spills), measured 2 % (FP32) and 5-9 % (BF16 / FP8) faster on a
+// 1M-point graph than with the ~160-170 registers of a one-block minimum.  PQ keeps the
+// one-block minimum (up to 255 registers).
+__global__ void __launch_bounds__(128, (MODE == kModePQ) ? 1 : 4)
     k_search_warp(const SearchParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
