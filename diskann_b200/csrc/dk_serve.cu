@@ -108,8 +108,13 @@ void release(dk_server* s) {
   delete s;
 }
 
+constexpr uint64_t kRetired = ~0ull;  // a context's ticket entry already collected
+
 // Collect finished requests into the request table: each request as soon as its done flag
-// is up, and a context's remaining ones when its launch has ended.
+// is up, and a context's remaining ones when its launch has ended.  A collected request's
+// entry in its context is retired at once: its table slot may be freed and handed to a newer
+// request (ticket + queue_depth) on another context while this launch still runs, and that
+// slot must not be matched against this launch's flags again.
 int32_t reap(dk_server* s) {
   const uint32_t max_k = s->cfg.max_k, depth = s->cfg.queue_depth;
   for (Context& c : s->ctx) {
@@ -122,8 +127,8 @@ int32_t reap(dk_server* s) {
     const float* d = reinterpret_cast<const float*>(c.host + s->off_d);
     const dk_search_stats* st = reinterpret_cast<const dk_search_stats*>(c.host + s->off_st);
     for (size_t i = 0; i < c.tickets.size(); ++i) {
+      if (c.tickets[i] == kRetired) continue;
       const uint32_t r = (uint32_t)(c.tickets[i] % depth);
-      if (s->state[r] != kInFlight) continue;
       if (!ended && flag[i] != c.seq) continue;
       std::atomic_thread_fence(std::memory_order_acquire);
       const uint32_t k = s->req_k[r];
@@ -131,6 +136,7 @@ int32_t reap(dk_server* s) {
       memcpy(&s->res_dists[(size_t)r * max_k], d + i * max_k, 4ull * k);
       s->res_stats[r] = st[i];
       s->state[r] = kDone;
+      c.tickets[i] = kRetired;
     }
     if (ended) {
       c.tickets.clear();

@@ -154,3 +154,28 @@ def test_native_replay_matches_the_oracle_under_load():
         np.testing.assert_array_equal(ids[i, : ks[i]], oi[0])
         np.testing.assert_array_equal(dists[i, : ks[i]].view(np.uint32), od[0].view(np.uint32))
     srv.close()
+
+
+def test_replay_far_above_capacity_returns_each_request_its_own_results():
+    """Every request arrives at once with a small queue depth and short and long requests in
+    the same launches: requests finish and free their table slots while their launch still
+    runs, and newer requests take those slots on other contexts.  Each must still get its own
+    results (the reference's single-query search, bit for bit)."""
+    v, a, d, n = random_index(4000, 64, 24, seed=21)
+    q = queries_like(v[:n], 300, seed=22)
+    orc = O.OracleIndex(v, a, d, n, O.METRIC_L2)
+    srv = SearchServer(GpuProvider(v, a, d, n, Metric.L2), FullPrecision(), max_k=10,
+                       max_l=300, queue_depth=16, streams=4)
+    rng = np.random.default_rng(23)
+    m = 3000
+    ks = np.full(m, 10)
+    ls = rng.choice([10, 20, 300], size=m)
+    lat, ids, dists = srv.replay(q, ks, ls, np.zeros(m), want_results=True)
+    srv.close()
+    want = {int(l): orc.search(q, 10, int(l), 1, O.STRATEGY_FULL_PRECISION) for l in (10, 20, 300)}
+    rows = np.arange(m) % q.shape[0]
+    exp_ids = np.stack([want[int(ls[i])][0][rows[i]] for i in range(m)])
+    exp_d = np.stack([want[int(ls[i])][1][rows[i]] for i in range(m)])
+    wrong = np.flatnonzero((ids[:, :10] != exp_ids).any(1))
+    assert wrong.size == 0, f"{wrong.size} of {m} requests got other results, first {wrong[:5]}"
+    np.testing.assert_array_equal(dists[:, :10].view(np.uint32), exp_d.view(np.uint32))
