@@ -60,6 +60,14 @@ WORKLOADS = {
                     nq=10_000, R=64, l_build=128, alpha=1.2, pq_chunks=0, pq_train=0, k=10,
                     l_sweep=[128, 192, 256], strategies=["fp32", "bf16", "fp8"],
                     seed=0xD15CA77 + 3),
+    # The large FP8 + PQ shape: 20M x 384, a zero-centred 1,024-component mixture (means
+    # U[-50, 50]^384, sigma 8) with every row scaled to unit length, inner product, R = 32,
+    # PQ 48 x 256.  Held in memory, not cached on disk (31 GB of rows; one rank).
+    "ip20m": dict(n=20_000_000, dim=384, normalized=True, metric=1, comps=1024, sigma=8.0,
+                  mean_range=(-50.0, 50.0), clip=(-255.0, 255.0),
+                  nq=10_000, R=32, l_build=100, alpha=1.2, pq_chunks=48, pq_train=100_000, k=10,
+                  l_sweep=[64, 100, 128, 192, 256, 384, 512],
+                  strategies=["fp32", "fp8", "hybrid"], seed=0xD15CA77 + 5, cache=False),
     # The served-stream shape: 10M x 96 mixture of 1,024 components, R = 48.
     "mix10m": dict(n=10_000_000, dim=96, comps=1024, sigma=8.0, nq=10_000, R=48, l_build=100,
                    alpha=1.2, pq_chunks=0, pq_train=0, k=10, l_sweep=[64, 128, 256, 512],
@@ -89,23 +97,31 @@ def prepare(name: str, rank: int, cache_root: str):
     from diskann_b200.groundtruth import knn_f64
 
     w = WORKLOADS[name]
+    cache = w.get("cache", True)
+    if not cache and rank != 0:
+        raise RuntimeError(f"workload {name} is prepared in memory by one rank only")
     cdir = os.path.join(cache_root, f"{name}-{workload_key(w)}")
     ready = os.path.join(cdir, "READY")
+    fresh = {}
     if rank != 0:
         t0 = time.time()
         while not os.path.exists(ready):
             if time.time() - t0 > 1800:
                 raise TimeoutError("rank 0 did not finish preparing the workload")
             time.sleep(1.0)
-    elif not os.path.exists(ready):
-        os.makedirs(cdir, exist_ok=True)
+    elif not cache or not os.path.exists(ready):
         t0 = time.time()
-        if w.get("normalized"):
+        if w.get("normalized") and not w["comps"]:
             base, queries = datasets.normalized_gaussian(w["n"], w["dim"], w["seed"],
                                                          n_queries=w["nq"])
         else:
-            base, queries = datasets.gaussian_mixture(w["n"], w["dim"], w["comps"], w["sigma"],
-                                                      seed=w["seed"], n_queries=w["nq"])
+            base, queries = datasets.gaussian_mixture(
+                w["n"], w["dim"], w["comps"], w["sigma"], seed=w["seed"],
+                mean_range=w.get("mean_range", (0.0, 100.0)), clip=w.get("clip", (0.0, 255.0)),
+                n_queries=w["nq"])
+            if w.get("normalized"):
+                datasets.normalize_rows(base)
+                datasets.normalize_rows(queries)
         log(f"[prepare] data {time.time() - t0:.1f}s")
         t0 = time.time()
         import torch
@@ -117,24 +133,31 @@ def prepare(name: str, rank: int, cache_root: str):
                                                   device=dev)
         log(f"[prepare] vamana build ({'GPU searches' if dev is not None else 'host'}) "
             f"{time.time() - t0:.1f}s, mean degree {deg[:n].mean():.1f}")
-        np.save(os.path.join(cdir, "vectors.npy"), vectors)
-        np.save(os.path.join(cdir, "queries.npy"), queries)
-        np.save(os.path.join(cdir, "adj.npy"), adj)
-        np.save(os.path.join(cdir, "deg.npy"), deg)
+        del base  # the first n rows of `vectors` are the same rows
+        fresh = dict(vectors=vectors, queries=queries, adj=adj, deg=deg, pq=None)
         if w["pq_chunks"]:
             t0 = time.time()
-            pq = graph.build_pq(vectors, w["pq_chunks"], w["pq_train"], seed=w["seed"])
+            fresh["pq"] = graph.build_pq(vectors, w["pq_chunks"], w["pq_train"], seed=w["seed"])
             log(f"[prepare] pq {time.time() - t0:.1f}s")
-            np.save(os.path.join(cdir, "pq_offsets.npy"), pq.offsets)
-            np.save(os.path.join(cdir, "pq_pivots.npy"), pq.pivots)
-            np.save(os.path.join(cdir, "pq_codes.npy"), pq.codes)
         t0 = time.time()
-        gt, _ = knn_f64(base, queries, w["k"], int(metric_of(w)))
+        fresh["gt"], _ = knn_f64(vectors[:n], queries, w["k"], int(metric_of(w)))
+        if dev is not None:
+            torch.cuda.empty_cache()
         log(f"[prepare] float64 ground truth {time.time() - t0:.1f}s")
-        np.save(os.path.join(cdir, "gt.npy"), gt)
-        with open(ready, "w") as f:
-            f.write("ok\n")
+        if cache:
+            os.makedirs(cdir, exist_ok=True)
+            for key in ("vectors", "queries", "adj", "deg", "gt"):
+                np.save(os.path.join(cdir, f"{key}.npy"), fresh[key])
+            if fresh["pq"] is not None:
+                np.save(os.path.join(cdir, "pq_offsets.npy"), fresh["pq"].offsets)
+                np.save(os.path.join(cdir, "pq_pivots.npy"), fresh["pq"].pivots)
+                np.save(os.path.join(cdir, "pq_codes.npy"), fresh["pq"].codes)
+            with open(ready, "w") as f:
+                f.write("ok\n")
     out = dict(w=w, n=w["n"])
+    if fresh:
+        out.update(fresh)
+        return out
     for key in ("vectors", "queries", "adj", "deg", "gt"):
         out[key] = np.load(os.path.join(cdir, f"{key}.npy"))
     if w["pq_chunks"]:
@@ -701,14 +724,23 @@ def choose_l_on_cpu(data, strategy):
     return w["l_sweep"][-1]
 
 
+def describe_data(w):
+    if w.get("normalized") and not w["comps"]:
+        return "isotropic Gaussian rows scaled to unit length"
+    lo, hi = w.get("mean_range", (0.0, 100.0))
+    mix = f"Gaussian mixture ({w['comps']} comp, means U[{lo:g}, {hi:g}], sigma {w['sigma']})"
+    return mix + (", rows scaled to unit length" if w.get("normalized") else "")
+
+
 def config_of(w, name, l, strategy):
     return {
-        "workload": (f"{name}: {w['n']:,} x {w['dim']} f32 Gaussian mixture ({w['comps']} comp, "
-                     f"sigma {w['sigma']}), Vamana R={w['R']} L_build={w['l_build']} "
+        "workload": (f"{name}: {w['n']:,} x {w['dim']} f32 {describe_data(w)}, "
+                     f"{metric_of(w).name}, Vamana R={w['R']} L_build={w['l_build']} "
                      f"alpha={w['alpha']}" + (f", PQ {w['pq_chunks']}x256" if w["pq_chunks"] else "")
                      + f", {w['nq']:,} queries, k={w['k']}, L={l}, strategy={strategy}"),
         "n_points": w["n"], "dim": w["dim"], "queries_per_step": w["nq"], "k": w["k"], "L": l,
-        "strategy": strategy, "metric": "L2", "l2_flush": "256 MiB write before every step",
+        "strategy": strategy, "metric": metric_of(w).name,
+        "l2_flush": "256 MiB write before every step",
         "parallelism": "replicas",
     }
 

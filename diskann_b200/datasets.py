@@ -6,7 +6,7 @@
   point (synthetic.rs:295-348; provider.rs:323-338).
 * ``gaussian_mixture`` / ``normalized_gaussian``: the benchmark workloads' vector shapes
   (a seeded Gaussian mixture clipped to [0, 255], or isotropic Gaussian rows normalised to
-  unit length).
+  unit length); ``normalize_rows`` scales a mixture's rows to unit length in place.
 """
 
 from __future__ import annotations
@@ -84,3 +84,12 @@ def normalized_gaussian(n: int, dim: int, seed: int, n_queries: int = 0):
     base = draw(n, np.random.default_rng(seed + 1))
     queries = draw(n_queries, np.random.default_rng(seed + 2)) if n_queries else None
     return base, queries
+
+
+def normalize_rows(x: np.ndarray, chunk: int = 1 << 16) -> np.ndarray:
+    """Scale every row of the float32 array ``x`` to unit L2 norm, in place, a chunk of rows
+    at a time (no full-size temporary).  Returns ``x``."""
+    for s in range(0, x.shape[0], chunk):
+        blk = x[s:s + chunk]
+        blk /= np.linalg.norm(blk, axis=1, keepdims=True)
+    return x

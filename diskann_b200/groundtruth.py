@@ -19,10 +19,11 @@ def knn_f64(base: np.ndarray, queries: np.ndarray, k: int, metric: int = 2,
     if device.startswith("cuda") and not torch.cuda.is_available():
         device = "cpu"
     dev = torch.device(device)
-    B = torch.as_tensor(np.ascontiguousarray(base), device=dev).to(torch.float64)
+    # The base stays in its own type on the device; each chunk is widened to float64 (exact)
+    # when it is used, so a large base needs its own size in memory, not twice that.
+    B = torch.as_tensor(np.ascontiguousarray(base), device=dev)
     Q = torch.as_tensor(np.ascontiguousarray(queries), device=dev).to(torch.float64)
     n = B.shape[0]
-    bn = (B * B).sum(1)
     out_i = np.empty((Q.shape[0], k), np.uint32)
     out_d = np.empty((Q.shape[0], k), np.float64)
     for q0 in range(0, Q.shape[0], query_block):
@@ -31,16 +32,17 @@ def knn_f64(base: np.ndarray, queries: np.ndarray, k: int, metric: int = 2,
         best_d = None
         best_i = None
         for b0 in range(0, n, base_chunk):
-            x = B[b0:b0 + base_chunk]
+            x = B[b0:b0 + base_chunk].to(torch.float64)
+            bn = (x * x).sum(1)
             dot = q @ x.T
             if metric == 2:
-                d = qn - 2.0 * dot + bn[b0:b0 + base_chunk][None, :]
+                d = qn - 2.0 * dot + bn[None, :]
             elif metric == 1:
                 d = -dot
             elif metric == 3:
                 d = 1.0 - dot
             else:
-                d = 1.0 - dot / (qn.sqrt() * bn[b0:b0 + base_chunk].sqrt()[None, :]).clamp_min(1e-300)
+                d = 1.0 - dot / (qn.sqrt() * bn.sqrt()[None, :]).clamp_min(1e-300)
             kk = min(k, d.shape[1])
             vd, vi = torch.topk(d, kk, dim=1, largest=False)
             vi = vi + b0
