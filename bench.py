@@ -61,12 +61,12 @@ WORKLOADS = {
                     l_sweep=[128, 192, 256], strategies=["fp32", "bf16", "fp8"],
                     seed=0xD15CA77 + 3),
     # The large FP8 + PQ shape: 20M x 384, a zero-centred 1,024-component mixture (means
-    # U[-50, 50]^384, sigma 8) with every row scaled to unit length, inner product, R = 32,
-    # PQ 48 x 256.  Held in memory, not cached on disk (31 GB of rows; one rank).
+    # U[-50, 50]^384, sigma 8) with every row scaled to unit length, inner product, R = 32
+    # (L_build 200), PQ 48 x 256.  Held in memory, not cached on disk (31 GB of rows; one rank).
     "ip20m": dict(n=20_000_000, dim=384, normalized=True, metric=1, comps=1024, sigma=8.0,
                   mean_range=(-50.0, 50.0), clip=(-255.0, 255.0),
-                  nq=10_000, R=32, l_build=100, alpha=1.2, pq_chunks=48, pq_train=100_000, k=10,
-                  l_sweep=[64, 100, 128, 192, 256, 384, 512],
+                  nq=10_000, R=32, l_build=200, alpha=1.2, pq_chunks=48, pq_train=100_000, k=10,
+                  l_sweep=[64, 100, 128, 192, 256, 384, 512, 768],
                   strategies=["fp32", "fp8", "hybrid"], seed=0xD15CA77 + 5, cache=False),
     # The served-stream shape: 10M x 96 mixture of 1,024 components, R = 48.
     "mix10m": dict(n=10_000_000, dim=96, comps=1024, sigma=8.0, nq=10_000, R=48, l_build=100,
@@ -602,9 +602,14 @@ def next_rows(data, threads, build=True):
     _, d10, _ = idx.search(Knn(k, 50), FullPrecision(), q)
     radius = float(np.median(d10[:, k - 1]))
     rp = Range(50, radius)
+    from diskann_b200 import STATS_DTYPE
+
+    rbuf = (np.empty((nq, 2000), np.uint32), np.empty((nq, 2000), np.float32),
+            np.zeros(nq, STATS_DTYPE))  # caller-owned result arrays, reused
     res = {}
-    t = _median_time(lambda: res.__setitem__("r", idx.range_search(rp, q, capacity=2000)))
-    counts = res["r"][1]["result_count"]
+    t = _median_time(lambda: res.__setitem__(
+        "r", idx.range_search_arrays(rp, q, capacity=2000, out=rbuf)))
+    counts = res["r"][2]["result_count"]
     t0 = time.perf_counter()
     for i in range(sample):
         o.range_search(q[i], 50, radius, capacity=2000)
@@ -612,13 +617,13 @@ def next_rows(data, threads, build=True):
     out["range"] = {"qps": round(nq / t, 1), "cpu_qps": round(cpu, 1), "cpu_cores": 1,
                     "starting_l": 50, "radius": round(radius, 3),
                     "mean_results": round(float(counts.mean()), 2),
-                    "second_round": round(float((res["r"][1]["flags"] & 2).astype(bool).mean()), 3)}
+                    "second_round": round(float((res["r"][2]["flags"] & 2).astype(bool).mean()), 3)}
 
     # Paged: one session per query, l_value 50, three pages of 10.
     def paged():
         ps = idx.paged_search(q, 50)
         for _ in range(3):
-            ps.next_page(k)
+            ps.next_page_arrays(k)
         ps.close()
     t = _median_time(paged)
     t0 = time.perf_counter()

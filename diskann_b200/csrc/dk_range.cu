@@ -24,7 +24,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstring>
 #include <string>
+#include <vector>
 
 #include "dk_kernels.cuh"
 
@@ -286,6 +288,38 @@ int32_t launch_range_search(dk_index* ix, const float* queries, uint64_t qstride
   return DK_OK;
 }
 
+// Packs each query's filled result slots (row pitch `capacity`) into one contiguous run at
+// offs[q] (the exclusive prefix sum of the result counts), so that the copy to host memory
+// carries the results only, not every query's full capacity.  One warp per query.
+__global__ void __launch_bounds__(256) k_pack_results(const uint32_t* ids, const float* d,
+                                                      uint32_t capacity, const uint64_t* offs,
+                                                      uint32_t nq, uint32_t* pid, float* pd) {
+  const uint32_t lane = threadIdx.x & 31u, wpb = blockDim.x >> 5;
+  for (uint32_t q = blockIdx.x * wpb + (threadIdx.x >> 5); q < nq; q += gridDim.x * wpb) {
+    const uint64_t o = offs[q];
+    const uint32_t c = (uint32_t)(offs[q + 1] - o);
+    for (uint32_t j = lane; j < c; j += 32u) {
+      pid[o + j] = ids[(size_t)q * capacity + j];
+      pd[o + j] = d[(size_t)q * capacity + j];
+    }
+  }
+}
+
+// Spreads `total` packed values, stored at the tail of the caller's nq x capacity array, into
+// the heads of their rows, in place.  Rows are visited in order and each moves to or before
+// its packed position (the results of rows q.. number at most (nq - q) * capacity), and a
+// row's moved values end where the next row's packed values begin, so nothing unread is
+// overwritten.
+template <typename T>
+void spread_in_place(T* a, uint32_t nq, uint32_t capacity, const std::vector<uint64_t>& offs) {
+  const uint64_t total = offs[nq];
+  T* packed = a + (uint64_t)nq * capacity - total;
+  for (uint32_t q = 0; q < nq; ++q) {
+    const uint64_t c = offs[q + 1] - offs[q];
+    if (c) memmove(a + (uint64_t)q * capacity, packed + offs[q], c * sizeof(T));
+  }
+}
+
 }  // namespace
 
 extern "C" int32_t dk_range_search_device(dk_index* ix, const float* queries,
@@ -344,11 +378,52 @@ extern "C" int32_t dk_range_search(dk_index* ix, const float* queries, uint64_t 
                              reinterpret_cast<uint32_t*>(buf + off_ids),
                              reinterpret_cast<float*>(buf + off_d),
                              reinterpret_cast<dk_search_stats*>(buf + off_st), s);
-    if (rc == DK_OK) {
-      e = cudaMemcpyAsync(ids, buf + off_ids, obytes, cudaMemcpyDeviceToHost, s);
-      if (e == cudaSuccess) e = cudaMemcpyAsync(dists, buf + off_d, obytes, cudaMemcpyDeviceToHost, s);
-      if (e == cudaSuccess && stats)
-        e = cudaMemcpyAsync(stats, buf + off_st, (size_t)nq * sizeof(dk_search_stats), cudaMemcpyDeviceToHost, s);
+    // The counts first; then only the filled slots come back (packed on the device), unless
+    // the rows are mostly full anyway.
+    std::vector<dk_search_stats> st(nq);
+    if (rc == DK_OK)
+      e = cudaMemcpyAsync(st.data(), buf + off_st, (size_t)nq * sizeof(dk_search_stats),
+                          cudaMemcpyDeviceToHost, s);
+    if (rc == DK_OK && e == cudaSuccess) e = cudaStreamSynchronize(s);
+    std::vector<uint64_t> offs(nq + 1, 0);
+    if (rc == DK_OK && e == cudaSuccess) {
+      for (uint32_t q = 0; q < nq; ++q) offs[q + 1] = offs[q] + std::min(st[q].result_count, capacity);
+      const uint64_t total = offs[nq];
+      if (2 * total >= (uint64_t)nq * capacity) {
+        e = cudaMemcpyAsync(ids, buf + off_ids, obytes, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(dists, buf + off_d, obytes, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      } else if (total) {
+        const size_t p_offs = 0, p_ids = ((size_t)(nq + 1) * 8 + 255) / 256 * 256;
+        const size_t p_d = p_ids + (total * 4 + 255) / 256 * 256, p_total = p_d + total * 4;
+        unsigned char* pk = nullptr;
+        e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&pk), p_total, ix->pool, s);
+        if (e == cudaSuccess) {
+          e = cudaMemcpyAsync(pk + p_offs, offs.data(), (size_t)(nq + 1) * 8, cudaMemcpyHostToDevice, s);
+          if (e == cudaSuccess) {
+            const uint32_t blocks = std::min<uint32_t>((nq + 7) / 8, 4096);
+            k_pack_results<<<blocks, 256, 0, s>>>(
+                reinterpret_cast<const uint32_t*>(buf + off_ids),
+                reinterpret_cast<const float*>(buf + off_d), capacity,
+                reinterpret_cast<const uint64_t*>(pk + p_offs), nq,
+                reinterpret_cast<uint32_t*>(pk + p_ids), reinterpret_cast<float*>(pk + p_d));
+            e = cudaGetLastError();
+          }
+          const uint64_t tail = (uint64_t)nq * capacity - total;
+          if (e == cudaSuccess)
+            e = cudaMemcpyAsync(ids + tail, pk + p_ids, total * 4, cudaMemcpyDeviceToHost, s);
+          if (e == cudaSuccess)
+            e = cudaMemcpyAsync(dists + tail, pk + p_d, total * 4, cudaMemcpyDeviceToHost, s);
+          cudaFreeAsync(pk, s);
+          const cudaError_t ep = cudaStreamSynchronize(s);
+          if (e == cudaSuccess) e = ep;
+          if (e == cudaSuccess) {
+            spread_in_place(ids, nq, capacity, offs);
+            spread_in_place(dists, nq, capacity, offs);
+          }
+        }
+      }
+      if (e == cudaSuccess && stats) memcpy(stats, st.data(), (size_t)nq * sizeof(dk_search_stats));
     }
   }
   cudaFreeAsync(buf, s);

@@ -386,24 +386,41 @@ class DiskANNIndex:
         """Range search of host queries (FullPrecision, ``dk_range_search``).  Returns
         ``(results, stats)``: per query a ``(ids, dists)`` pair of its results, and the stats
         array (flags bit 1: second round ran; bit 2: results reached the capacity)."""
+        ids, dists, stats = self.range_search_arrays(params, queries, capacity)
+        return _rows(ids, dists, stats), stats
+
+    def range_search_arrays(self, params: Range, queries, capacity: int | None = None,
+                            out=None):
+        """:meth:`range_search` returning ``(ids, dists, stats)`` arrays: ``(nq, capacity)``
+        rows whose first ``stats["result_count"]`` entries are the results (the rest are
+        unspecified).  ``out``: optional caller-owned ``(ids, dists, stats)`` arrays of those
+        shapes and types, reused instead of allocating."""
         q = np.ascontiguousarray(np.atleast_2d(queries), dtype=np.float32)
         if q.shape[1] != self.provider.dim:
             raise ANNError(Status.DIMENSION_MISMATCH, f"query dim {q.shape[1]} != {self.provider.dim}")
         cap = capacity or params.max_returned or self.provider.num_points
         cap = max(cap, params.starting_l, params.max_returned or 0)
         nq = q.shape[0]
-        ids = np.empty((nq, cap), dtype=np.uint32)
-        dists = np.empty((nq, cap), dtype=np.float32)
-        stats = np.zeros(nq, dtype=STATS_DTYPE)
+        if out is None:
+            ids = np.empty((nq, cap), dtype=np.uint32)
+            dists = np.empty((nq, cap), dtype=np.float32)
+            stats = np.zeros(nq, dtype=STATS_DTYPE)
+        else:
+            ids, dists, stats = out
+            if (ids.shape != (nq, cap) or ids.dtype != np.uint32 or dists.shape != (nq, cap)
+                    or dists.dtype != np.float32 or stats.shape != (nq,)
+                    or stats.dtype != STATS_DTYPE or not all(
+                        a.flags.c_contiguous for a in (ids, dists, stats))):
+                raise ANNError(Status.INVALID_ARGUMENT,
+                               "out must be contiguous (nq, capacity) uint32 / float32 arrays "
+                               "and an (nq,) stats array")
         _check(_native.load().dk_range_search(
             self.provider.handle, q.ctypes.data, q.shape[1], nq, params.starting_l,
             params.beam_width, params.radius,
             float("nan") if params.inner_radius is None else params.inner_radius,
             params.initial_slack, params.range_slack, params.max_returned or 0, cap,
             ids.ctypes.data, dists.ctypes.data, stats.ctypes.data))
-        out = [(ids[i, : stats[i]["result_count"]], dists[i, : stats[i]["result_count"]])
-               for i in range(nq)]
-        return out, stats
+        return ids, dists, stats
 
     def paged_search(self, queries, l_value: int, init_ids=None, queue_capacity: int = 0):
         """Start a paged search for each query (FullPrecision, ``dk_paged_search_create``;
@@ -430,6 +447,12 @@ class DiskANNIndex:
             params.k_value, params.l_value, params.beam_width, ids.data_ptr(), dists.data_ptr(),
             stats.data_ptr(), ctypes.c_void_p(handle),
         ))
+
+
+def _rows(ids, dists, stats):
+    """Per row, the ``(ids, dists)`` of its first ``result_count`` entries."""
+    counts = stats["result_count"].tolist()
+    return [(ids[i, :c], dists[i, :c]) for i, c in enumerate(counts)]
 
 
 class PagedSearch:
@@ -463,14 +486,18 @@ class PagedSearch:
         self._h = handle
 
     def next_page(self, k: int):
+        ids, dists, stats = self.next_page_arrays(k)
+        return _rows(ids, dists, stats), stats
+
+    def next_page_arrays(self, k: int):
+        """:meth:`next_page` returning ``(ids, dists, stats)`` arrays: ``(nq, k)`` rows whose
+        first ``stats["result_count"]`` entries are each session's page."""
         ids = np.empty((self.nq, max(k, 1)), dtype=np.uint32)
         dists = np.empty((self.nq, max(k, 1)), dtype=np.float32)
         stats = np.zeros(self.nq, dtype=STATS_DTYPE)
         _check(_native.load().dk_paged_search_next(self._h, k, ids.ctypes.data,
                                                    dists.ctypes.data, stats.ctypes.data))
-        pages = [(ids[i, : stats[i]["result_count"]], dists[i, : stats[i]["result_count"]])
-                 for i in range(self.nq)]
-        return pages, stats
+        return ids, dists, stats
 
     def close(self) -> None:
         if getattr(self, "_h", None):

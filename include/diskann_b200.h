@@ -168,7 +168,9 @@ int32_t dk_search_device(dk_index* index, int32_t strategy, const float* queries
  * radius * range_slack; results are the start-point-free entries with
  * inner_radius < distance <= radius, in the reference's order.  inner_radius NaN = none;
  * max_returned 0 = unlimited.  Each query gets `capacity` (>= starting_l, >= max_returned) output
- * slots: result_count in stats says how many are filled; with max_returned unlimited, flags
+ * slots: result_count in stats says how many are filled (this host entry point copies back the
+ * filled slots only and leaves the rest of each row unspecified; the device entry point pads
+ * them with id 0xFFFFFFFF, distance +inf); with max_returned unlimited, flags
  * bit 2 marks a query whose results reached the capacity (possibly incomplete); flags bit 1:
  * the second round ran.  Stats follow the reference (cmps of the first round; with a second
  * round, hops counts the first round twice, as the reference's scratch counter does). */

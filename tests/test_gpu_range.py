@@ -121,3 +121,29 @@ def test_range_device_entry_point_matches_host_entry_point():
         np.testing.assert_array_equal(ids_h[i, :c], host[i][0])
         np.testing.assert_array_equal(d_h[i, :c].view(np.uint32), host[i][1].view(np.uint32))
         assert int(st_h[i]["cmps"]) == int(hst[i]["cmps"])
+
+
+@pytest.mark.parametrize("capacity,radius_rank", [(40, 39), (4000, 5), (4000, 60)])
+def test_host_copy_of_filled_slots_only(capacity, radius_rank):
+    """The host entry point copies back only each query's filled slots (packed on the device,
+    spread in place into the caller's rows) unless the rows are mostly full; either way every
+    row's results equal the oracle's, also into reused caller-owned arrays."""
+    from diskann_b200 import STATS_DTYPE
+
+    v, a, d, n = random_index(3000, 64, 24, seed=78, max_degree=31)
+    q = queries_like(v[:n], 64, seed=9)
+    idx = DiskANNIndex(GpuProvider(v, a, d, n, Metric.L2))
+    orc = O.OracleIndex(v, a, d, n, O.METRIC_L2)
+    _, d0, _ = orc.search(q[:1], 60, 80, 1)
+    p = Range(40, float(d0[0, radius_rank]))
+    out = (np.full((64, capacity), 7, np.uint32), np.full((64, capacity), 7.0, np.float32),
+           np.zeros(64, STATS_DTYPE))
+    for _ in range(2):
+        ids, dists, st = idx.range_search_arrays(p, q, capacity=capacity, out=out)
+        assert ids is out[0] and dists is out[1] and st is out[2]
+        for i in range(64):
+            oi, od, ost = orc.range_search(q[i], p.starting_l, p.radius, capacity=capacity)
+            c = int(st[i]["result_count"])
+            assert c == int(ost["result_count"][0])
+            np.testing.assert_array_equal(ids[i, :c], oi)
+            np.testing.assert_array_equal(dists[i, :c].view(np.uint32), od.view(np.uint32))
