@@ -144,6 +144,6 @@ def test_host_copy_of_filled_slots_only(capacity, radius_rank):
         for i in range(64):
             oi, od, ost = orc.range_search(q[i], p.starting_l, p.radius, capacity=capacity)
             c = int(st[i]["result_count"])
-            assert c == int(ost["result_count"][0])
+            assert c == int(np.asarray(ost["result_count"]).reshape(-1)[0])
             np.testing.assert_array_equal(ids[i, :c], oi)
             np.testing.assert_array_equal(dists[i, :c].view(np.uint32), od.view(np.uint32))
