@@ -123,7 +123,7 @@ def test_range_device_entry_point_matches_host_entry_point():
         assert int(st_h[i]["cmps"]) == int(hst[i]["cmps"])
 
 
-@pytest.mark.parametrize("capacity,radius_rank", [(40, 39), (4000, 5), (4000, 60)])
+@pytest.mark.parametrize("capacity,radius_rank", [(40, 39), (4000, 5), (4000, 59)])
 def test_host_copy_of_filled_slots_only(capacity, radius_rank):
     """The host entry point copies back only each query's filled slots (packed on the device,
     spread in place into the caller's rows) unless the rows are mostly full; either way every
