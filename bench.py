@@ -61,12 +61,12 @@ WORKLOADS = {
                     l_sweep=[128, 192, 256], strategies=["fp32", "bf16", "fp8"],
                     seed=0xD15CA77 + 3),
     # The large FP8 + PQ shape: 20M x 384, a zero-centred 1,024-component mixture (means
-    # U[-50, 50]^384, sigma 8) with every row scaled to unit length, inner product, R = 32,
-    # PQ 48 x 256.  Held in memory, not cached on disk (31 GB of rows; one rank).
+    # U[-50, 50]^384, sigma 8) with every row scaled to unit length, inner product, R = 32
+    # (L_build 200), PQ 48 x 256.  Held in memory, not cached on disk (31 GB of rows; one rank).
     "ip20m": dict(n=20_000_000, dim=384, normalized=True, metric=1, comps=1024, sigma=8.0,
                   mean_range=(-50.0, 50.0), clip=(-255.0, 255.0),
-                  nq=10_000, R=32, l_build=100, alpha=1.2, pq_chunks=48, pq_train=100_000, k=10,
-                  l_sweep=[64, 100, 128, 192, 256, 384, 512],
+                  nq=10_000, R=32, l_build=200, alpha=1.2, pq_chunks=48, pq_train=100_000, k=10,
+                  l_sweep=[64, 100, 128, 192, 256, 384, 512, 768],
                   strategies=["fp32", "fp8", "hybrid"], seed=0xD15CA77 + 5, cache=False),
     # The served-stream shape: 10M x 96 mixture of 1,024 components, R = 48.
     "mix10m": dict(n=10_000_000, dim=96, comps=1024, sigma=8.0, nq=10_000, R=48, l_build=100,
