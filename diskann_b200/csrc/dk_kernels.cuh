@@ -1816,8 +1816,10 @@ uint32_t plan_query_smem(SearchParams& P, bool pq, bool with_hash);
 // Fill the index and list fields of `P` for k, L (capacity L + F) and the beam width.
 void base_params(const dk_index* ix, int32_t strategy, uint32_t k, uint32_t l, uint32_t beam,
                  SearchParams& P);
-// Visited-set size estimates (largest, mean) for the queue capacity in `P`.
-void visited_estimates(dk_index* ix, const SearchParams& P, double& est, double& est_mean);
+// Visited-set size estimates (largest, mean) for the queue capacity in `P`.  `absorb`: first
+// take in the values the last launch staged (false: read the index's current estimate only).
+void visited_estimates(dk_index* ix, const SearchParams& P, double& est, double& est_mean,
+                       bool absorb = true);
 // Plan a warp-per-query launch (shared level, global level, warps per CTA, and a grid of at
 // most `max_warps` warps, capped at the resident maximum); returns a dk_status.
 int32_t plan_warp(dk_index* ix, SearchParams& P, LaunchPlan& L, int mode, double est,

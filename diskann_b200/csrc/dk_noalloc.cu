@@ -5,10 +5,17 @@
 // holds on every GPU that loads it until the process exits.  No counterpart in the reference.
 //
 // Set-up: the first call on a device, made with that device current, looks the array's device
-// address up with cudaGetSymbolAddress and keeps it for later calls.  The array is shared by
-// every call on a device and keeps the last call's contents; each call clears the one word
-// that must start at zero (the work counter), and the kernels clear their own visited tables
-// and bitmaps.  Calls whose work overlaps on the GPU race on the array.
+// address up with cudaGetSymbolAddress and keeps it for later calls.  With CUDA's lazy module
+// loading the array's memory is committed when that look-up loads the module, so the set-up
+// call (nq = 0 is enough) belongs before the caller's allocator reserves the GPU's memory; a
+// set-up that finds no room fails with DK_ERR_CUDA.  The array is shared by every call on a
+// device and keeps the last call's contents; each call clears the one word that must start at
+// zero (the work counter), and the kernels clear their own visited tables and bitmaps.  Calls
+// whose work overlaps on the GPU race on the array.  The visited tables are sized from the
+// index's visited-size estimate, which only dk_search_device updates; this entry point reads it.
+// The spill pass runs at most one CTA per SM here, with at most half of the room one CTA's
+// tables leave (dk_search_device allows up to eight per SM), so batches in which many queries
+// spill finish more slowly through this entry point.
 
 #include <cuda_runtime.h>
 
@@ -109,9 +116,12 @@ extern "C" int32_t dk_search_device_noalloc(dk_index* ix, int32_t strategy, cons
   P.out_ids = ids;
   P.out_dists = dists;
   P.stats = stats;
-  P.hint = ix->hint_dev;
+  // The visited tables are sized from the estimate that dk_search_device keeps on this index;
+  // this entry point only reads it (it records nothing into, and resets nothing of, the
+  // index's estimate words, which a dk_search_device on another stream may be using).
+  P.hint = nullptr;
   double est = 0, est_mean = 0;
-  dk::visited_estimates(ix, P, est, est_mean);
+  dk::visited_estimates(ix, P, est, est_mean, /*absorb=*/false);
   int max_optin = 0, sms = 0;
   cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ix->device);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ix->device);
@@ -175,9 +185,6 @@ extern "C" int32_t dk_search_device_noalloc(dk_index* ix, int32_t strategy, cons
   L.p2 = P2;
   L.spill_ctas = spill_ctas;
   if (e == cudaSuccess) e = dk::dispatch(ix->metric, L, mode, stream);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(ix->hint_stage, ix->hint_dev, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(ix->hint_dev, 0, 3 * sizeof(uint32_t), stream);
   if (e != cudaSuccess)
     return fail(DK_ERR_CUDA, std::string("search launch: ") + cudaGetErrorString(e));
   return DK_OK;

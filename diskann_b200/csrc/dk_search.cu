@@ -98,7 +98,8 @@ void base_params(const dk_index* ix, int32_t strategy, uint32_t k, uint32_t l, u
   P.list_cap = std::max(std::max(beam * ix->max_degree, P.cap), ix->f);
 }
 
-void visited_estimates(dk_index* ix, const SearchParams& P, double& est, double& est_mean) {
+void visited_estimates(dk_index* ix, const SearchParams& P, double& est, double& est_mean,
+                       bool absorb) {
   // |visited| equals the comparison count, which for a given graph grows about linearly with
   // L + F.  The largest and the mean ratio are learned from previous launches on this index
   // (see dk_index::hint_dev); before any launch the prior is half the reference's own
@@ -108,10 +109,12 @@ void visited_estimates(dk_index* ix, const SearchParams& P, double& est, double&
   double ratio = 0.5 * 1.1 * 1.3 * ix->max_degree;
   double mean_ratio = ratio;
   {
-    volatile uint32_t* h = ix->hint_stage;  // written by the previous launch's async copy
-    const uint32_t seen = h[0], sum = h[1], cnt = h[2];
-    if (seen) ix->hint_max = seen;
-    if (cnt) ix->hint_mean = (uint32_t)(((uint64_t)sum + cnt - 1) / cnt);
+    if (absorb) {
+      volatile uint32_t* h = ix->hint_stage;  // written by the previous launch's async copy
+      const uint32_t seen = h[0], sum = h[1], cnt = h[2];
+      if (seen) ix->hint_max = seen;
+      if (cnt) ix->hint_mean = (uint32_t)(((uint64_t)sum + cnt - 1) / cnt);
+    }
     if (ix->hint_max) ratio = (double)ix->hint_max / 256.0 * 1.15;
     if (ix->hint_mean) mean_ratio = (double)ix->hint_mean / 256.0;
   }

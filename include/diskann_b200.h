@@ -258,7 +258,14 @@ int32_t dk_inmem_search(dk_index* index, const void* queries, uint64_t query_str
  * every GPU that loads the library holds until the process exits.  No counterpart in the
  * reference.
  *  - Set-up: the first call on a device, made with that device current, looks up the array's
- *    device address; make that first call (nq = 0 is enough) before any stream capture.
+ *    device address; make that first call (nq = 0 is enough) before any stream capture.  With
+ *    CUDA's lazy module loading the array's memory is committed by that look-up, so make the
+ *    set-up call before your own allocator reserves the GPU's memory; a set-up that finds no
+ *    room returns DK_ERR_CUDA (out of memory).
+ *  - Visited tables are sized from the index's visited-size estimate, which only
+ *    dk_search_device calls update; this entry point reads it and never changes it.
+ *  - The spill pass (queries whose visited set outgrows the tables) runs at most one CTA per
+ *    SM here, against up to eight in dk_search_device, so spill-heavy batches run slower.
  *  - Limit: a search whose scratch would not fit the array (one spill bitmap of (N+F)/8
  *    bytes plus one CTA's visited tables at least) is refused with DK_ERR_UNSUPPORTED and a
  *    message giving the bytes it needs; large batches run with fewer warps when not all of
