@@ -91,6 +91,24 @@ void orc_bruteforce_f64(const float* base, uint32_t n, uint32_t dim, uint32_t st
                         uint32_t* ids_out, double* dists_out);
 void orc_pq_table(const orc_index* ix, const float* query, float* table_out);
 
+// Graph construction (build.cpp): the reference's insert rules with a deterministic batch
+// schedule; ids num_points.. are the frozen start points (their vectors must be set).
+typedef struct orc_build_params {
+  uint32_t pruned_degree;  // R
+  uint32_t max_degree;     // slot width (list length allowed before a back edge prunes)
+  uint32_t l_build;
+  float alpha;
+  uint32_t max_backedges;
+  uint32_t max_occlusion;  // 0 = 750
+  uint32_t num_threads;    // 0 = all hardware threads
+  uint32_t max_batch;      // 0 = max(64, num_points / 64)
+} orc_build_params;
+int32_t orc_build_vamana(const float* vectors, uint32_t vector_stride, uint32_t num_points,
+                         uint32_t num_frozen, uint32_t dim, int32_t metric,
+                         const orc_build_params* params, uint32_t* adjacency,
+                         uint32_t adjacency_stride, uint32_t* degrees);
+uint32_t orc_medoid(const float* vectors, uint32_t stride, uint32_t n, uint32_t dim);
+
 #ifdef __cplusplus
 }
 #endif

@@ -60,6 +60,19 @@ class Stats(ctypes.Structure):
     ]
 
 
+class BuildParams(ctypes.Structure):
+    _fields_ = [
+        ("pruned_degree", ctypes.c_uint32),
+        ("max_degree", ctypes.c_uint32),
+        ("l_build", ctypes.c_uint32),
+        ("alpha", ctypes.c_float),
+        ("max_backedges", ctypes.c_uint32),
+        ("max_occlusion", ctypes.c_uint32),
+        ("num_threads", ctypes.c_uint32),
+        ("max_batch", ctypes.c_uint32),
+    ]
+
+
 STATS_DTYPE = np.dtype(
     [("cmps", np.uint32), ("hops", np.uint32), ("result_count", np.uint32), ("flags", np.uint32)]
 )
@@ -67,7 +80,7 @@ STATS_DTYPE = np.dtype(
 
 def build() -> str:
     """Compile the oracle (g++) if it is missing or stale; return the library path."""
-    src = [os.path.join(_HERE, f) for f in ("oracle.cpp", "oracle.h", "Makefile")]
+    src = [os.path.join(_HERE, f) for f in ("oracle.cpp", "build.cpp", "oracle.h", "Makefile")]
     if os.path.exists(_LIB_PATH) and all(
         os.path.getmtime(_LIB_PATH) >= os.path.getmtime(s) for s in src
     ):
@@ -99,6 +112,13 @@ def lib():
                 ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int32,
                 ctypes.c_void_p, ctypes.c_void_p,
             ]
+            L.orc_build_vamana.restype = ctypes.c_int32
+            L.orc_build_vamana.argtypes = [
+                ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                ctypes.c_int32, ctypes.POINTER(BuildParams), ctypes.c_void_p, ctypes.c_uint32,
+                ctypes.c_void_p]
+            L.orc_medoid.restype = ctypes.c_uint32
+            L.orc_medoid.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]
             L.orc_pq_table.restype = None
             L.orc_pq_table.argtypes = [ctypes.POINTER(_Index), ctypes.c_void_p, ctypes.c_void_p]
             L.orc_range_search.restype = ctypes.c_int32
@@ -283,3 +303,30 @@ def bruteforce_f64(base, queries, k, metric):
     lib().orc_bruteforce_f64(_ptr(base), base.shape[0], base.shape[1], base.shape[1], _ptr(q),
                              q.shape[0], k, metric, _ptr(ids), _ptr(d))
     return ids, d
+
+
+def medoid(base) -> int:
+    """The reference's medoid rule (medoid.rs:15-45) restated (build.cpp)."""
+    base = np.ascontiguousarray(base, dtype=np.float32)
+    return int(lib().orc_medoid(_ptr(base), base.shape[1], base.shape[0], base.shape[1]))
+
+
+def build_vamana(base, metric, pruned_degree, l_build, alpha=1.2, max_degree=None,
+                 backedge_ratio=1.0, num_threads=0, max_batch=0):
+    """Graph construction restated on the CPU (build.cpp), with the medoid row copied to the
+    frozen start point (id N).  Returns ``(vectors, adjacency, degrees, n)`` in the layout of
+    ``diskann_b200.graph.build_vamana``, whose result it must equal."""
+    base = np.ascontiguousarray(base, dtype=np.float32)
+    n, dim = base.shape
+    med = medoid(base)
+    vectors = np.vstack([base, base[med:med + 1]])
+    md = max_degree or int(np.float32(pruned_degree) * np.float32(1.3))
+    adjacency = np.zeros((n + 1, md), np.uint32)
+    degrees = np.zeros(n + 1, np.uint32)
+    p = BuildParams(pruned_degree, md, l_build, alpha, int(np.ceil(backedge_ratio * pruned_degree)),
+                    0, num_threads, max_batch)
+    rc = lib().orc_build_vamana(_ptr(vectors), dim, n, 1, dim, int(metric), ctypes.byref(p),
+                                _ptr(adjacency), md, _ptr(degrees))
+    if rc != 0:
+        raise ValueError(f"oracle build failed with status {rc}")
+    return vectors, adjacency, degrees, n

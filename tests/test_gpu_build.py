@@ -38,3 +38,21 @@ def test_device_build_long_lists(monkeypatch, env):
     v1, a1, d1, n1 = graph.build_vamana(base, device=0, **kw)
     np.testing.assert_array_equal(d0, d1)
     np.testing.assert_array_equal(a0, a1)
+
+
+@pytest.mark.parametrize("metric,dim", [(Metric.L2, 128), (Metric.INNER_PRODUCT, 96)])
+def test_device_build_equals_oracle_build(metric, dim):
+    """The device build against the oracle's independent restatement of the construction rules
+    (oracle/build.cpp): the identical graph, on enough points that most batches run on the GPU."""
+    from oracle import oracle as O
+
+    if metric == Metric.L2:
+        base, _ = datasets.gaussian_mixture(20000, dim, 32, 8.0, seed=dim + 1)
+    else:
+        base, _ = datasets.normalized_gaussian(20000, dim, seed=dim + 1)
+    kw = dict(pruned_degree=32, l_build=50, alpha=1.2, max_batch=2048)
+    v0, a0, d0, n0 = graph.build_vamana(base, metric=metric, device=0, **kw)
+    v1, a1, d1, n1 = O.build_vamana(base, int(metric), **kw)
+    np.testing.assert_array_equal(v0, v1)
+    np.testing.assert_array_equal(d0, d1)
+    np.testing.assert_array_equal(a0, a1)
