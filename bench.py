@@ -74,6 +74,7 @@ WORKLOADS = {
                    strategies=["fp32", "bf16", "fp8"], seed=0xD15CA77 + 4),
 }
 TARGET_RECALL = 0.95
+PARITY_QUERIES = 1000
 METRIC_NAME = "QPS at recall@10>=0.95"
 
 
@@ -91,16 +92,24 @@ def workload_key(w: dict) -> str:
     return hashlib.sha1(json.dumps(w, sort_keys=True).encode()).hexdigest()[:12]
 
 
-def prepare(name: str, rank: int, cache_root: str):
-    """Generate (or load from the per-box cache) data, graph, PQ and ground truth."""
-    from diskann_b200 import datasets, graph
+def prepare(name: str, rank: int, cache_root: str, builder: str = "library"):
+    """Generate (or load from the per-box cache) data, graph, PQ and ground truth.
+
+    ``builder="library"``: the graph is built by this library (GPU-searched batches when a GPU
+    is present) and PQ is trained by it.  ``builder="oracle"``: the CPU reference arm, which
+    must not load this library: the graph comes from the oracle's restatement of the same
+    construction (the identical graph, tests/test_oracle_build.py and test_gpu_build.py), the
+    medoid from the oracle's restatement of the reference's rule, and no PQ is built (that arm
+    times the FullPrecision search only).  Each builder keeps its own cache."""
+    from diskann_b200 import datasets
     from diskann_b200.groundtruth import knn_f64
 
     w = WORKLOADS[name]
     cache = w.get("cache", True)
     if not cache and rank != 0:
         raise RuntimeError(f"workload {name} is prepared in memory by one rank only")
-    cdir = os.path.join(cache_root, f"{name}-{workload_key(w)}")
+    tag = "" if builder == "library" else f"-{builder}"
+    cdir = os.path.join(cache_root, f"{name}-{workload_key(w)}{tag}")
     ready = os.path.join(cdir, "READY")
     fresh = {}
     if rank != 0:
@@ -126,16 +135,30 @@ def prepare(name: str, rank: int, cache_root: str):
         t0 = time.time()
         import torch
 
-        # Larger batches search on the GPU when there is one: the same graph as the host build.
         dev = 0 if torch.cuda.is_available() else None
-        vectors, adj, deg, n = graph.build_vamana(base, metric=metric_of(w), pruned_degree=w["R"],
-                                                  l_build=w["l_build"], alpha=w["alpha"],
-                                                  device=dev)
-        log(f"[prepare] vamana build ({'GPU searches' if dev is not None else 'host'}) "
-            f"{time.time() - t0:.1f}s, mean degree {deg[:n].mean():.1f}")
+        if builder == "oracle":
+            from oracle import oracle as orc
+
+            vectors, adj, deg, n = orc.build_vamana(base, int(metric_of(w)), w["R"],
+                                                    w["l_build"], w["alpha"])
+            how = "oracle, host threads"
+        else:
+            from diskann_b200 import graph
+
+            # Larger batches search on the GPU when there is one: the same graph as the host
+            # build.
+            vectors, adj, deg, n = graph.build_vamana(base, metric=metric_of(w),
+                                                      pruned_degree=w["R"],
+                                                      l_build=w["l_build"], alpha=w["alpha"],
+                                                      device=dev)
+            how = "GPU searches" if dev is not None else "host"
+        log(f"[prepare] vamana build ({how}) {time.time() - t0:.1f}s, "
+            f"mean degree {deg[:n].mean():.1f}")
         del base  # the first n rows of `vectors` are the same rows
         fresh = dict(vectors=vectors, queries=queries, adj=adj, deg=deg, pq=None)
-        if w["pq_chunks"]:
+        if w["pq_chunks"] and builder == "library":
+            from diskann_b200 import graph
+
             t0 = time.time()
             fresh["pq"] = graph.build_pq(vectors, w["pq_chunks"], w["pq_train"], seed=w["seed"])
             log(f"[prepare] pq {time.time() - t0:.1f}s")
@@ -160,7 +183,7 @@ def prepare(name: str, rank: int, cache_root: str):
         return out
     for key in ("vectors", "queries", "adj", "deg", "gt"):
         out[key] = np.load(os.path.join(cdir, f"{key}.npy"))
-    if w["pq_chunks"]:
+    if w["pq_chunks"] and os.path.exists(os.path.join(cdir, "pq_codes.npy")):
         from diskann_b200 import PQData
 
         out["pq"] = PQData(np.load(os.path.join(cdir, "pq_offsets.npy")),
@@ -500,8 +523,22 @@ def run_ours(args, data, rank, world):
         fp32_alg = algorithmic_bytes(st32, w, fp32_row["L"], mean_deg, "fp32")
         fp32_row = dict(fp32_row, roofline_frac=round(
             fp32_alg * fp32_row["qps"] / nq / 1e9 / peak, 4))
+    # GPU results of the first PARITY_QUERIES queries for the strategies whose results are
+    # defined bit for bit by the reference's search (FullPrecision, Hybrid), each at its own L;
+    # the CPU-baseline leg runs the oracle on the same queries and compares.
+    parity_gpu = {}
+    if world == 1:
+        for name in ("fp32", "hybrid"):
+            if name in table:
+                lp = table[name]["L"]
+                search(Knn(k, lp), strategies[name])
+                torch.cuda.synchronize()
+                m = min(PARITY_QUERIES, nq)
+                parity_gpu[name] = (lp, ids[:m].cpu().numpy().view(np.uint32).copy(),
+                                    dists[:m].cpu().numpy().copy(),
+                                    stats_array(stats[:m].cpu().numpy().view(np.uint32)))
     return dict(value=value, ms_per_step=ms_per_step, recall=rec, L=chosen, strategy=head,
-                strategies=table, fp32=fp32_row, serving=serving,
+                strategies=table, fp32=fp32_row, serving=serving, parity_gpu=parity_gpu,
                 e2e=dict(value=world * nq / e2e_s, unit="queries/s",
                          h2d_bytes_per_step=int(queries.nbytes),
                          d2h_bytes_per_step=int(nq * k * 8 + nq * 16)),
@@ -826,7 +863,7 @@ def main():
         # sample of the query batch.
         if rank != 0:
             return 0
-        data = prepare(args.workload, 0, args.cache)
+        data = prepare(args.workload, 0, args.cache, builder="oracle")
         w = data["w"]
         l = choose_l_on_cpu(data, "fp32")
         sample = min(w["nq"], 4000)
@@ -874,6 +911,21 @@ def main():
             cpu = {"value": round(qps, 1), "unit": "queries/s", "cores": threads, "kind": "port",
                    "sample": f"{reps} x {sample} queries, {threads} threads, "
                              f"{cpu_strat} L={cpu_l}, {cpu_model()}"}
+            # Parity: the oracle on the first PARITY_QUERIES queries against the GPU's results.
+            parity = {}
+            o = oracle_index(data)
+            for name, (lp, gi, gd, gs) in r["parity_gpu"].items():
+                m = gi.shape[0]
+                oi, od, ost = o.search(data["queries"][:m], w["k"], lp, 1, oracle_strategy(name),
+                                       threads=threads)
+                parity[name] = {
+                    "L": lp, "of": int(m),
+                    "ids_equal": int((gi == oi).all(1).sum()),
+                    "dist_bits_equal": int((gd.view(np.uint32) == od.view(np.uint32)).all(1).sum()),
+                    "cmps_equal": int((gs["cmps"] == ost["cmps"]).sum()),
+                    "hops_equal": int((gs["hops"] == ost["hops"]).sum()),
+                    "result_count_equal": int((gs["result_count"] == ost["result_count"]).sum())}
+            log(f"[ours] parity vs oracle {parity}")
         line = {
             "metric": METRIC_NAME, "value": round(r["value"], 1), "unit": "queries/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -882,13 +934,18 @@ def main():
             "config": config_of(w, args.workload, r["L"], r["strategy"]),
             "recall_at_10": round(r["recall"], 4), "strategies": r["strategies"],
             "fp32_path_at_target": r["fp32"],
-            "vs_fp32_path": (round(r["value"] / world / r["fp32"]["qps"], 3)
-                             if r["fp32"] else None),
+            # Each precision form's QPS over the plain FP32 path's, both at the smallest L of
+            # the sweep reaching the recall target (or their last L when it is not reached).
+            "precision_vs_fp32": {n: round(row["qps"] / r["fp32"]["qps"], 3)
+                                  for n, row in r["strategies"].items()
+                                  if n in ("bf16", "fp8") and r["fp32"]},
             "serving": r["serving"],
             "e2e": {k: (round(v, 1) if isinstance(v, float) else v) for k, v in r["e2e"].items()},
             "gpu_launches": r["gpu_launches"], "roofline": r["roofline"], "cpu_baseline": cpu,
             "clocks": r["clocks"], "search_stats": r["stats"],
         }
+        if cpu is not None:
+            line["parity"] = parity
         if world == 1 and not args.no_next_rows:
             line["next_rows"] = next_rows(data, threads)
             log(f"[ours] next rows {line['next_rows']}")
