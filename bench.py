@@ -68,6 +68,13 @@ WORKLOADS = {
                   nq=10_000, R=32, l_build=200, alpha=1.2, pq_chunks=48, pq_train=100_000, k=10,
                   l_sweep=[64, 100, 128, 192, 256, 384, 512, 768],
                   strategies=["fp32", "fp8", "hybrid"], seed=0xD15CA77 + 5, cache=False),
+    # A 2M-point slice of the 20M x 384 shape (same generator family, R = 32, L_build 200):
+    # small enough to prepare in about a minute, for sweeps of the wide-row, long-search regime.
+    "ip2m384": dict(n=2_000_000, dim=384, normalized=True, metric=1, comps=1024, sigma=8.0,
+                    mean_range=(-50.0, 50.0), clip=(-255.0, 255.0),
+                    nq=10_000, R=32, l_build=200, alpha=1.2, pq_chunks=0, pq_train=0, k=10,
+                    l_sweep=[64, 100, 128, 192, 256, 384, 512],
+                    strategies=["fp32", "bf16", "fp8"], seed=0xD15CA77 + 6),
     # The served-stream shape: 10M x 96 mixture of 1,024 components, R = 48.
     "mix10m": dict(n=10_000_000, dim=96, comps=1024, sigma=8.0, nq=10_000, R=48, l_build=100,
                    alpha=1.2, pq_chunks=0, pq_train=0, k=10, l_sweep=[64, 128, 256, 512],
@@ -75,6 +82,7 @@ WORKLOADS = {
 }
 TARGET_RECALL = 0.95
 PARITY_QUERIES = 1000
+SERVE_P99_BOUND_MS = 2.0
 METRIC_NAME = "QPS at recall@10>=0.95"
 
 
@@ -307,6 +315,13 @@ def max_rel_dist_error(ids, dists, data, metric):
     """Largest relative error of the returned float32 distances against the same pairs'
     distances in float64 (the precision forms rerank with exact FP32 rows, so this is the
     FP32 rounding of the final distances)."""
+    rel = rel_dist_errors(ids, dists, data, metric)
+    return None if rel is None else float(rel.max())
+
+
+def rel_dist_errors(ids, dists, data, metric):
+    """Relative error of each (query row, id) pair's float32 distance against float64 over the
+    original float32 rows (0 for invalid ids); None when no id is valid."""
     import torch
 
     from diskann_b200 import Metric
@@ -314,7 +329,7 @@ def max_rel_dist_error(ids, dists, data, metric):
     valid = ids != 0xFFFFFFFF
     if not valid.any():
         return None
-    q = torch.from_numpy(data["queries"]).cuda().double()
+    q = torch.from_numpy(data["queries"][: ids.shape[0]]).cuda().double()
     rows = torch.from_numpy(data["vectors"][np.where(valid, ids, 0).astype(np.int64)]).cuda().double()
     if metric == Metric.L2:
         d = ((rows - q[:, None, :]) ** 2).sum(-1)
@@ -327,7 +342,7 @@ def max_rel_dist_error(ids, dists, data, metric):
     got = torch.from_numpy(dists.astype(np.float64)).cuda()
     rel = (got - d).abs() / d.abs().clamp_min(1e-12)
     rel = torch.where(torch.from_numpy(valid).cuda(), rel, torch.zeros_like(rel))
-    return float(rel.max())
+    return rel.cpu().numpy()
 
 
 def stats_array(st):
@@ -445,6 +460,17 @@ def run_ours(args, data, rank, world):
         err = max_rel_dist_error(ids.cpu().numpy().view(np.uint32), dists.cpu().numpy(), data,
                                  metric_of(w))
         row["max_rel_dist_err_vs_f64"] = None if err is None else float(f"{err:.3g}")
+        if name in ("bf16", "fp8"):
+            # The traversal's own (low-precision) distances of the returned pairs, before the
+            # FP32 rerank, against float64 over the original rows (first 1,000 queries).
+            m = min(PARITY_QUERIES, nq)
+            sid = ids[:m].cpu().numpy().view(np.uint32).copy()
+            lp = idx.score(strat, queries[:m], sid)
+            rel = rel_dist_errors(sid, lp, data, metric_of(w))
+            if rel is not None:
+                row["scoring_rel_err_vs_f64"] = {"median": float(f"{np.median(rel):.3g}"),
+                                                 "p99": float(f"{np.quantile(rel, 0.99):.3g}"),
+                                                 "max": float(f"{rel.max():.3g}")}
         row["qps"] = round(timed(Knn(k, row["L"]), strat), 1)
         table[name] = row
         log(f"[ours] {name}: {row}")
@@ -500,15 +526,35 @@ def run_ours(args, data, rank, world):
             e2e_t.append(t1 - t0)
     e2e_s = max_over_ranks(float(np.mean(e2e_t)) * 1e3, world) / 1e3
 
-    # Serving: Poisson arrivals replayed through dk_server_* at several offered rates, and a
-    # mixed-k/L stream (N=1 only).
+    # Serving (N=1 only): per strategy, Poisson arrivals replayed through dk_server_* at
+    # offered rates doubling from 250k requests/s until the server saturates (achieved below
+    # 90 % of offered, or p99 above SERVE_P99_BOUND_MS); capacity = the highest achieved rate
+    # whose p99 stays within the bound.  Plus the mixed-k/L stream at 100k requests/s.
     serving = None
     if world == 1 and not args.no_serving:
-        serving = [serve_latency(provider, strategy, queries, gt, k, chosen, rate, args.serve_seconds)
-                   for rate in (10_000.0, 100_000.0, 500_000.0, 1_000_000.0)]
-        serving.append(serve_latency(provider, strategy, queries, gt, k, chosen, 100_000.0,
-                                     args.serve_seconds, mixed=True))
-        log(f"[ours] serving {serving}")
+        serving = {}
+        for name in ("fp32", "bf16", "fp8"):
+            if name not in table:
+                continue
+            st_obj, ls = strategies[name], table[name]["L"]
+            rows, cap = [], 0.0
+            rate = 250_000.0
+            while rate <= 8_000_000.0:
+                secs = min(args.serve_seconds, 2_000_000.0 / rate)
+                row = serve_latency(provider, st_obj, queries, gt, k, ls, rate, secs)
+                rows.append(row)
+                ok = row["p99_ms"] <= SERVE_P99_BOUND_MS
+                if ok:
+                    cap = max(cap, row["achieved_qps"])
+                if not ok or row["achieved_qps"] < 0.9 * rate:
+                    break
+                rate *= 2.0
+            mixed = serve_latency(provider, st_obj, queries, gt, k, ls, 100_000.0,
+                                  args.serve_seconds, mixed=True)
+            serving[name] = {"L": ls, "p99_bound_ms": SERVE_P99_BOUND_MS,
+                             "capacity_qps": round(cap, 1), "rates": rows, "mixed": mixed}
+            log(f"[ours] serving {name}: capacity {cap:.0f} req/s at p99 <= "
+                f"{SERVE_P99_BOUND_MS} ms; {rows} mixed {mixed}")
 
     mean_deg = float(data["deg"][: data["n"]].mean())
     alg = algorithmic_bytes(stats_np, w, chosen, mean_deg, head)

@@ -25,6 +25,7 @@ EXPORTED_SYMBOLS = (
     "dk_search",
     "dk_search_device",
     "dk_search_device_noalloc",
+    "dk_score_candidates",
     "dk_range_search",
     "dk_range_search_device",
     "dk_paged_search_create",
@@ -36,6 +37,7 @@ EXPORTED_SYMBOLS = (
     "dk_server_create",
     "dk_server_submit",
     "dk_server_poll",
+    "dk_server_cancel",
     "dk_server_replay",
     "dk_server_get_info",
     "dk_server_destroy",
@@ -112,6 +114,8 @@ class ServerConfig(ctypes.Structure):
         ("queue_depth", ctypes.c_uint32),
         ("max_slots", ctypes.c_uint32),
         ("streams", ctypes.c_uint32),
+        ("pad", ctypes.c_uint32),
+        ("memory_bytes", ctypes.c_uint64),
     ]
 
 
@@ -123,6 +127,8 @@ class ServerInfo(ctypes.Structure):
         ("pad", ctypes.c_uint32),
         ("device_bytes", ctypes.c_uint64),
         ("launches", ctypes.c_uint64),
+        ("memory_bytes", ctypes.c_uint64),
+        ("reserved_bytes", ctypes.c_uint64),
     ]
 
 
@@ -181,6 +187,8 @@ def load():
         L.dk_inmem_search.argtypes = [vp, vp, u64, u32, u32, u32, u32, vp, vp, vp]
         L.dk_search_device_noalloc.restype = i32
         L.dk_search_device_noalloc.argtypes = [vp, i32, vp, u64, u32, u32, u32, u32, vp, vp, vp, vp]
+        L.dk_score_candidates.restype = i32
+        L.dk_score_candidates.argtypes = [vp, i32, vp, u64, u32, vp, u32, vp, vp]
         L.dk_server_create.restype = i32
         L.dk_server_create.argtypes = [vp, ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]
         L.dk_server_submit.restype = i32
@@ -188,6 +196,8 @@ def load():
         L.dk_server_poll.restype = i32
         L.dk_server_poll.argtypes = [vp, u64, vp, vp, vp]
         L.dk_server_replay.restype = i32
+        L.dk_server_cancel.restype = i32
+        L.dk_server_cancel.argtypes = [vp, u64]
         L.dk_server_replay.argtypes = [vp, vp, u64, u32, vp, vp, vp, u32, vp, vp, vp]
         L.dk_server_get_info.restype = i32
         L.dk_server_get_info.argtypes = [vp, ctypes.POINTER(ServerInfo)]

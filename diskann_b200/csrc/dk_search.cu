@@ -95,7 +95,9 @@ void base_params(const dk_index* ix, int32_t strategy, uint32_t k, uint32_t l, u
   P.cap = l + ix->f;
   P.beam = beam;
   P.strategy = strategy;
-  P.list_cap = std::max(std::max(beam * ix->max_degree, P.cap), ix->f);
+  // One hop's candidates (or the start points).  The rerank of the queue (up to L + F entries)
+  // uses the queue's second buffer, free once the last merge is done.
+  P.list_cap = std::max(beam * ix->max_degree, ix->f);
 }
 
 void visited_estimates(dk_index* ix, const SearchParams& P, double& est, double& est_mean,
@@ -133,14 +135,15 @@ int32_t plan_warp(dk_index* ix, SearchParams& P, LaunchPlan& L, int mode, double
   // shared-memory budget; the global level takes what a longer search adds.
   P.hash_log2 = 0;
   const uint32_t base = plan_query_smem(P, pq, false);
-  // Per-warp budget (measured on the 1M x 128 workload): the kernels are fastest with a shared
-  // level holding ~1.1x the mean visited set at load 3/4 (12-20 KB per warp), which keeps
-  // nearly every probe out of the global level, rather than with more resident warps.  PQ
+  // Per-warp budget (measured on the 1M x 128 and 2M x 384 workloads): the kernels are fastest
+  // with a shared level holding ~1.1x the mean visited set at load 3/4 (12-32 KB per warp),
+  // which keeps nearly every probe out of the global level, rather than with more resident
+  // warps (2M x 384 at L = 512: 342k QPS with 20 KB per warp, 371k with 28 KB).  PQ
   // traversal keeps its ADC table and a minimal level.  DK_WARP_SMEM overrides.
   uint32_t dflt = 12288;
   if (mode != kModePQ) {
     dflt = base + (uint32_t)(4.0 * est_mean * 1.1 / 0.75);
-    dflt = std::min<uint32_t>(std::max<uint32_t>(dflt, 12288), 20480);
+    dflt = std::min<uint32_t>(std::max<uint32_t>(dflt, 12288), 32768);
   }
   const uint32_t budget = std::max<uint32_t>(env_u32("DK_WARP_SMEM", dflt), base + 1024);
   uint32_t slots = align_up((uint32_t)(est_mean * 1.3 / 0.75) + 1, 32);

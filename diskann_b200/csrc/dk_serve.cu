@@ -34,7 +34,7 @@ namespace {
 
 inline uint64_t round_up(uint64_t x, uint64_t a) { return (x + a - 1) / a * a; }
 
-enum : uint8_t { kFree = 0, kPending = 1, kInFlight = 2, kDone = 3 };
+enum : uint8_t { kFree = 0, kPending = 1, kInFlight = 2, kDone = 3, kCancelled = 4 };
 
 // One launch context.  Device buffer layout (each part 256-B aligned):
 // counter | kl[cap][2] | queries[cap][dim] | ids[cap][max_k] | dists[cap][max_k] |
@@ -66,7 +66,14 @@ struct dk_server {
   uint64_t host_bytes = 0;
   // Outstanding requests, indexed by ticket % queue_depth.
   std::vector<uint8_t> state;
+  std::vector<uint8_t> cancel;       // cancelled while in flight: its results are dropped
   std::vector<uint32_t> req_k, req_l;
+  std::vector<uint64_t> req_bytes;   // device memory reserved for the request's beam state
+  // Admission by device memory: every outstanding request reserves the bytes its beam state
+  // needs at its own L (beam_bytes); a request is admitted while the reservations fit
+  // `memory_bytes` (the device memory held for beam state).
+  uint64_t memory_bytes = 0, reserved_bytes = 0;
+  double visited_per_entry = 0;  // visited ids per queue entry (the index's learned ratio)
   std::vector<float> queries;       // queue_depth x dim
   std::vector<uint32_t> res_ids;    // queue_depth x max_k
   std::vector<float> res_dists;     // queue_depth x max_k
@@ -131,12 +138,16 @@ int32_t reap(dk_server* s) {
       const uint32_t r = (uint32_t)(c.tickets[i] % depth);
       if (!ended && flag[i] != c.seq) continue;
       std::atomic_thread_fence(std::memory_order_acquire);
+      c.tickets[i] = kRetired;
+      if (s->cancel[r]) {  // cancelled while in flight: its results are not kept
+        s->state[r] = kCancelled;
+        continue;
+      }
       const uint32_t k = s->req_k[r];
       memcpy(&s->res_ids[(size_t)r * max_k], ids + i * max_k, 4ull * k);
       memcpy(&s->res_dists[(size_t)r * max_k], d + i * max_k, 4ull * k);
       s->res_stats[r] = st[i];
       s->state[r] = kDone;
-      c.tickets[i] = kRetired;
     }
     if (ended) {
       c.tickets.clear();
@@ -199,6 +210,39 @@ int32_t progress(dk_server* s) {
   const int32_t rc = reap(s);
   if (rc != DK_OK) return rc;
   return launch_pending(s);
+}
+
+// Device memory a request's beam state needs at its L: its double-buffered queue of L + F
+// (distance, id) entries and its share of a visited table holding the expected visited set
+// (the index's learned visited-per-entry ratio times L + F, plus one hop's candidates) at
+// load 3/4.
+uint64_t beam_bytes(const dk_server* s, uint32_t l) {
+  const uint64_t cap = (uint64_t)l + s->ix->f;
+  const double visited = s->visited_per_entry * (double)cap +
+                         (double)s->cfg.beam_width * s->ix->max_degree + s->ix->f;
+  return 16ull * cap + 4ull * (uint64_t)(visited / 0.75 + 1.0);
+}
+
+// Admission of one more request needing `need` bytes: queue depth, then device memory.
+int32_t admit(const dk_server* s, uint64_t need) {
+  if (s->next_ticket - s->head >= s->cfg.queue_depth)
+    return fail(DK_ERR_ADMISSION, "queue_depth requests are outstanding");
+  if (s->reserved_bytes + need > s->memory_bytes)
+    return fail(DK_ERR_ADMISSION,
+                "the request's beam state (" + std::to_string(need) + " bytes) does not fit the " +
+                    "server's device memory for beam state (" + std::to_string(s->reserved_bytes) +
+                    " of " + std::to_string(s->memory_bytes) + " bytes reserved)");
+  return DK_OK;
+}
+
+// Free a collected (or cancelled) request's table slot and its memory reservation.
+void retire(dk_server* s, uint32_t r) {
+  s->state[r] = kFree;
+  s->cancel[r] = 0;
+  s->reserved_bytes -= s->req_bytes[r];
+  s->req_bytes[r] = 0;
+  const uint32_t depth = s->cfg.queue_depth;
+  while (s->head < s->next_ticket && s->state[s->head % depth] == kFree) ++s->head;
 }
 
 }  // namespace
@@ -283,7 +327,15 @@ extern "C" int32_t dk_server_create(dk_index* ix, const dk_server_config* cfg, d
     return fail(DK_ERR_OUT_OF_MEMORY, std::string("serving buffers: ") + cudaGetErrorString(e));
   }
   s->device_bytes = s->cfg.streams * s->dev_bytes + rerun_bytes;
+  // Beam-state memory: the visited tables of every context's warps (the queues live in
+  // shared memory beside them), unless the caller sets a smaller or larger budget.
+  s->visited_per_entry = std::max(0.0, (est_mean - (double)cfg->beam_width * ix->max_degree - ix->f) /
+                                           (double)P.cap);
+  s->memory_bytes = cfg->memory_bytes ? cfg->memory_bytes
+                                      : (uint64_t)s->cfg.streams * grid * per_cta_tables;
   s->state.assign(depth, kFree);
+  s->cancel.assign(depth, 0);
+  s->req_bytes.assign(depth, 0);
   s->req_k.assign(depth, 0);
   s->req_l.assign(depth, 0);
   s->queries.assign((size_t)depth * dim, 0.0f);
@@ -302,12 +354,15 @@ extern "C" int32_t dk_server_submit(dk_server* s, const float* query, uint32_t k
   if (k > s->cfg.max_k || l > s->cfg.max_l)
     return fail(DK_ERR_INVALID_ARGUMENT, "k or L above the server's max_k / max_l");
   std::lock_guard<std::mutex> lock(s->mu);
-  if (s->next_ticket - s->head >= s->cfg.queue_depth)
-    return fail(DK_ERR_ADMISSION, "queue_depth requests are outstanding");
+  const uint64_t need = beam_bytes(s, l);
+  const int32_t a = admit(s, need);
+  if (a != DK_OK) return a;
   const uint64_t t = s->next_ticket++;
   const uint32_t r = (uint32_t)(t % s->cfg.queue_depth);
   s->req_k[r] = k;
   s->req_l[r] = l;
+  s->req_bytes[r] = need;
+  s->reserved_bytes += need;
   memcpy(&s->queries[(size_t)r * s->ix->dim], query, 4ull * s->ix->dim);
   s->state[r] = kPending;
   s->pending.push_back(t);
@@ -325,10 +380,14 @@ extern "C" int32_t dk_server_poll(dk_server* s, uint64_t ticket, uint32_t* ids, 
   if (ticket >= s->next_ticket || ticket < s->head || s->state[r] == kFree)
     return fail(DK_ERR_NOT_FOUND, "unknown or already collected ticket");
   dk::DeviceGuard guard(s->ix->device);
-  if (s->state[r] != kDone) {
+  if (s->state[r] != kDone && s->state[r] != kCancelled) {
     const int32_t rc = progress(s);
     if (rc != DK_OK) return rc;
-    if (s->state[r] != kDone) return DK_ERR_NOT_READY;
+    if (s->state[r] != kDone && s->state[r] != kCancelled) return DK_ERR_NOT_READY;
+  }
+  if (s->state[r] == kCancelled) {
+    retire(s, r);
+    return fail(DK_ERR_CANCELLED, "the request was cancelled");
   }
   const uint32_t k = s->req_k[r];
   dk_search_stats st = s->res_stats[r];
@@ -357,8 +416,30 @@ extern "C" int32_t dk_server_poll(dk_server* s, uint64_t ticket, uint32_t* ids, 
     memcpy(dists, &s->res_dists[(size_t)r * max_k], 4ull * k);
   }
   if (stats) *stats = st;
-  s->state[r] = kFree;
-  while (s->head < s->next_ticket && s->state[s->head % depth] == kFree) ++s->head;
+  retire(s, r);
+  return DK_OK;
+}
+
+extern "C" int32_t dk_server_cancel(dk_server* s, uint64_t ticket) {
+  if (!s) return fail(DK_ERR_INVALID_ARGUMENT, "server is required");
+  std::lock_guard<std::mutex> lock(s->mu);
+  const uint32_t r = (uint32_t)(ticket % s->cfg.queue_depth);
+  if (ticket >= s->next_ticket || ticket < s->head || s->state[r] == kFree)
+    return fail(DK_ERR_NOT_FOUND, "unknown or already collected ticket");
+  switch (s->state[r]) {
+    case kPending:  // not launched yet: it never reaches the device
+      s->pending.erase(std::find(s->pending.begin(), s->pending.end(), ticket));
+      s->state[r] = kCancelled;
+      break;
+    case kInFlight:  // its launch finishes; the results are dropped when it is reaped
+      s->cancel[r] = 1;
+      break;
+    case kDone:
+      s->state[r] = kCancelled;
+      break;
+    default:
+      break;
+  }
   return DK_OK;
 }
 
@@ -376,6 +457,8 @@ extern "C" int32_t dk_server_replay(dk_server* s, const float* queries, uint64_t
       return fail(DK_ERR_INVALID_ARGUMENT, "k or L above the server's max_k / max_l");
     if (i && arrival_ns[i] < arrival_ns[i - 1])
       return fail(DK_ERR_INVALID_ARGUMENT, "arrival times must not decrease");
+    if (beam_bytes(s, ls[i]) > s->memory_bytes)
+      return fail(DK_ERR_ADMISSION, "a request's beam state exceeds the server's device memory for beam state");
   }
   const uint32_t max_k = s->cfg.max_k, depth = s->cfg.queue_depth, dim = s->ix->dim;
   std::vector<std::pair<uint64_t, uint32_t>> out;  // (ticket, request) in flight
@@ -392,11 +475,14 @@ extern "C" int32_t dk_server_replay(dk_server* s, const float* queries, uint64_t
     std::lock_guard<std::mutex> lock(s->mu);
     // Submit every request whose arrival time has come, while admission allows.
     const uint64_t now = now_ns();
-    while (next < n && arrival_ns[next] <= now && s->next_ticket - s->head < depth) {
+    while (next < n && arrival_ns[next] <= now && s->next_ticket - s->head < depth &&
+           s->reserved_bytes + beam_bytes(s, ls[next]) <= s->memory_bytes) {
       const uint64_t t = s->next_ticket++;
       const uint32_t r = (uint32_t)(t % depth);
       s->req_k[r] = ks[next];
       s->req_l[r] = ls[next];
+      s->req_bytes[r] = beam_bytes(s, ls[next]);
+      s->reserved_bytes += s->req_bytes[r];
       memcpy(&s->queries[(size_t)r * dim], queries + (size_t)(next % nq) * query_stride, 4ull * dim);
       s->state[r] = kPending;
       s->pending.push_back(t);
@@ -410,6 +496,13 @@ extern "C" int32_t dk_server_replay(dk_server* s, const float* queries, uint64_t
     for (size_t j = 0; j < out.size(); ++j) {
       const uint64_t t = out[j].first;
       const uint32_t i = out[j].second, r = (uint32_t)(t % depth);
+      if (s->state[r] == kCancelled) {  // cancelled by another thread: no results
+        const uint64_t fin = now_ns();
+        latency_ns[i] = fin > arrival_ns[i] ? fin - arrival_ns[i] : 0;
+        retire(s, r);
+        ++done;
+        continue;
+      }
       if (s->state[r] != kDone || (s->res_stats[r].flags & kFlagSpilled)) {
         if (s->state[r] == kDone) {
           // Spilled: collect through the exact re-run of dk_server_poll (lock released there).
@@ -422,11 +515,10 @@ extern "C" int32_t dk_server_replay(dk_server* s, const float* queries, uint64_t
       latency_ns[i] = fin > arrival_ns[i] ? fin - arrival_ns[i] : 0;
       if (ids) memcpy(ids + (size_t)i * max_k, &s->res_ids[(size_t)r * max_k], 4ull * ks[i]);
       if (dists) memcpy(dists + (size_t)i * max_k, &s->res_dists[(size_t)r * max_k], 4ull * ks[i]);
-      s->state[r] = kFree;
+      retire(s, r);
       ++done;
     }
     out.resize(w);
-    while (s->head < s->next_ticket && s->state[s->head % depth] == kFree) ++s->head;
     if (!keep.empty()) {
       // Rare: a request whose visited tables overflowed is re-run exactly by the batch path.
       std::vector<uint32_t> tid(max_k);
@@ -460,6 +552,8 @@ extern "C" int32_t dk_server_get_info(const dk_server* s, dk_server_info* info) 
   info->pad = 0;
   info->device_bytes = s->device_bytes;
   info->launches = s->launches;
+  info->memory_bytes = s->memory_bytes;
+  info->reserved_bytes = s->reserved_bytes;
   return DK_OK;
 }
 

@@ -449,6 +449,28 @@ class DiskANNIndex:
         ))
 
 
+    def score(self, strategy: _Strategy, queries, ids) -> np.ndarray:
+        """Distances each candidate gets from ``strategy``'s traversal scorer
+        (``dk_score_candidates``): ``queries`` (nq, D) float32, ``ids`` (nq, m) candidate ids;
+        returns (nq, m) float32 (NaN for an id outside the index)."""
+        import torch
+
+        q = np.ascontiguousarray(np.atleast_2d(queries), dtype=np.float32)
+        c = np.ascontiguousarray(np.atleast_2d(ids), dtype=np.uint32)
+        if c.shape[0] != q.shape[0]:
+            raise ValueError("one candidate row per query")
+        dev = torch.device("cuda", self.provider.device)
+        dq = torch.from_numpy(q).to(dev)
+        dc = torch.from_numpy(c.view(np.int32)).to(dev)
+        out = torch.empty(c.shape, dtype=torch.float32, device=dev)
+        stream = torch.cuda.current_stream(dev)
+        _check(_native.load().dk_score_candidates(
+            self.provider.handle, strategy.code, dq.data_ptr(), dq.stride(0), q.shape[0],
+            dc.data_ptr(), c.shape[1], out.data_ptr(), ctypes.c_void_p(stream.cuda_stream)))
+        torch.cuda.synchronize(dev)
+        return out.cpu().numpy()
+
+
 def _rows(ids, dists, stats):
     """Per row, the ``(ids, dists)`` of its first ``result_count`` entries."""
     counts = stats["result_count"].tolist()
@@ -520,10 +542,10 @@ class SearchServer:
 
     def __init__(self, provider: GpuProvider, strategy: _Strategy, max_k: int, max_l: int,
                  beam_width: int = 1, queue_depth: int = 1024, max_slots: int = 0,
-                 streams: int = 0):
+                 streams: int = 0, memory_bytes: int = 0):
         L = _native.load()
         cfg = _native.ServerConfig(strategy.code, max_k, max_l, beam_width, queue_depth,
-                                   max_slots, streams)
+                                   max_slots, streams, 0, memory_bytes)
         handle = ctypes.c_void_p()
         _check(L.dk_server_create(provider.handle, ctypes.byref(cfg), ctypes.byref(handle)))
         self._handle = handle
@@ -555,6 +577,11 @@ class SearchServer:
             return None
         _check(rc)
         return ids, dists, stats[0]
+
+    def cancel(self, ticket: int) -> None:
+        """Cancel an outstanding request (``dk_server_cancel``); its next ``poll`` raises
+        ``ANNError`` with status ``CANCELLED``."""
+        _check(_native.load().dk_server_cancel(self.handle, ticket))
 
     def wait(self, ticket: int, k: int, timeout_s: float = 30.0):
         """Poll until the request completes (``TimeoutError`` after ``timeout_s``)."""

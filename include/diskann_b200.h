@@ -160,6 +160,18 @@ int32_t dk_search_device(dk_index* index, int32_t strategy, const float* queries
                          uint32_t beam_width, uint32_t* ids, float* dists,
                          dk_search_stats* stats, void* stream);
 
+/* The distance each strategy scores a candidate with, for `nq` queries (rows of
+ * `query_stride` floats) and `per_query` candidate ids each (row-major, nq x per_query),
+ * written to `dists` (same shape).  DEVICE buffers, asynchronous on `stream`.  This is the
+ * accessor's per-candidate distance, batched (replaces the preprocessed query distance of
+ * diskann/src/utils/vector_repr.rs:48-93 for FullPrecision, bit-exact; the PQ QueryComputer of
+ * diskann-providers/src/model/pq/distance/dynamic.rs:64-84 for Hybrid / Quantized; for BF16 /
+ * FP8, which have no counterpart in the reference, the low-precision distance their traversal
+ * uses).  An id outside the index scores NaN. */
+int32_t dk_score_candidates(dk_index* index, int32_t strategy, const float* queries,
+                            uint64_t query_stride, uint32_t nq, const uint32_t* ids,
+                            uint32_t per_query, float* dists, void* stream);
+
 /* Range search with the FullPrecision strategy (replaces DiskANNIndex::search with the
  * reference's `Range` parameters, diskann/src/graph/search/range_search.rs:63-389): a first
  * greedy search with a queue of starting_l + F entries, then - when at least
@@ -292,7 +304,10 @@ int32_t dk_search_device_noalloc(dk_index* index, int32_t strategy, const float*
  * first one frees up.  dk_server_poll returns DK_OK once the request's results are in the
  * caller's buffers, else DK_ERR_NOT_READY; polling also reaps finished launches and starts
  * queued ones.  Admission: a submit is rejected with DK_ERR_ADMISSION while queue_depth
- * requests are outstanding (submitted, not yet collected).  All device memory (per-context
+ * requests are outstanding (submitted, not yet collected), or when the device memory its
+ * beam state needs at its own L (a double-buffered queue of L + F entries and a visited table
+ * for the expected visited set) does not fit the server's beam-state memory beside the
+ * reservations of the requests outstanding; a larger L therefore takes more of it.  All device memory (per-context
  * query, result and visited-table buffers) is taken at creation, sized from max_l, the
  * contexts' slots and the free device memory; no device code waits on the host.
  * A server's calls are serialised by an internal lock. */
@@ -306,6 +321,9 @@ typedef struct dk_server_config {
   uint32_t queue_depth;  /* outstanding requests accepted */
   uint32_t max_slots;    /* concurrent searches per launch (0 = all resident warps) */
   uint32_t streams;      /* launch contexts that overlap on the device (0 = 16) */
+  uint32_t pad;
+  uint64_t memory_bytes; /* device memory for beam state that admission fills (0 = the
+                            visited tables the server allocates) */
 } dk_server_config;
 
 typedef struct dk_server_info {
@@ -315,6 +333,8 @@ typedef struct dk_server_info {
   uint32_t pad;
   uint64_t device_bytes;     /* HBM held by the server */
   uint64_t launches;         /* kernel launches so far */
+  uint64_t memory_bytes;     /* device memory for beam state (admission budget) */
+  uint64_t reserved_bytes;   /* reserved by the outstanding requests now */
 } dk_server_info;
 
 int32_t dk_server_create(dk_index* index, const dk_server_config* config, dk_server** out);
@@ -322,6 +342,13 @@ int32_t dk_server_submit(dk_server* server, const float* query, uint32_t k, uint
                          uint64_t* ticket);
 int32_t dk_server_poll(dk_server* server, uint64_t ticket, uint32_t* ids, float* dists,
                        dk_search_stats* stats);
+/* Cancel an outstanding request (the serving analogue of dropping the reference's search
+ * future; its errors rank a cancellation as transient, diskann/src/error/ranked.rs:91-159):
+ * a queued request never reaches the device; one already on the device finishes its launch
+ * and its results are dropped.  The next dk_server_poll of the ticket returns
+ * DK_ERR_CANCELLED and frees its slot and memory reservation; the server stays usable.
+ * DK_ERR_NOT_FOUND for an unknown or collected ticket. */
+int32_t dk_server_cancel(dk_server* server, uint64_t ticket);
 /* Load-test driver (no counterpart in the reference; the role of its benchmark runner): replay
  * a request stream through the server from the calling host thread.  Request i uses query row
  * i % nq, k[i] and L[i], and is submitted arrival_ns[i] nanoseconds after the call starts (not

@@ -105,3 +105,45 @@ def test_missing_low_precision_copy_is_an_error():
         idx.search(Knn(5, 10), FP8(), v[:2])
     assert ei.value.status == Status.NO_LOW_PRECISION
     idx.search(Knn(5, 10), BF16(), v[:2])
+
+
+@pytest.mark.parametrize("metric", [Metric.L2, Metric.INNER_PRODUCT, Metric.COSINE_NORMALIZED,
+                                    Metric.COSINE])
+@pytest.mark.parametrize("dim", [32, 100, 128, 384])
+def test_candidate_scores_of_each_strategy(metric, dim):
+    """dk_score_candidates runs each strategy's traversal scorer: FullPrecision distances are
+    the oracle's bit for bit; BF16 / FP8 distances equal a float64 evaluation over the stored
+    (de-quantised) rows within 1e-5 of the terms' magnitude (FP32 accumulation); ids outside
+    the index score NaN."""
+    norm = metric != Metric.L2
+    v, a, d, n = random_index(2000, dim, 16, seed=dim + 3 * int(metric), normalize=norm,
+                              max_degree=20)
+    q = queries_like(v[:n], 12, seed=9, normalize=norm)
+    idx = DiskANNIndex(GpuProvider(v, a, d, n, metric, low_precision=("bf16", "fp8")))
+    rng = np.random.default_rng(dim)
+    cand = rng.integers(0, n + 1, size=(q.shape[0], 41)).astype(np.uint32)
+    cand[:, -1] = n + 7
+    full = idx.score(FullPrecision(), q, cand)
+    assert np.isnan(full[:, -1]).all()
+    for i in range(q.shape[0]):
+        for j in range(40):
+            exact = np.float32(O.distance(int(metric), q[i], v[cand[i, j]]))
+            assert full[i, j].view(np.uint32) == exact.view(np.uint32)
+    qd = q.astype(np.float64)[:, None, :]
+    for kind in ("bf16", "fp8"):
+        got = idx.score(STRATS[kind], q, cand)[:, :-1].astype(np.float64)
+        x = dequantised(v, kind).astype(np.float64)[cand[:, :-1]]
+        dot = (x * qd).sum(-1)
+        mag = (np.abs(x) * np.abs(qd)).sum(-1)
+        qq, xx = (qd ** 2).sum(-1), (x ** 2).sum(-1)
+        if metric == Metric.L2:
+            want, tol = qq + xx - 2 * dot, 1e-5 * (qq + xx + 2 * mag)
+        elif metric == Metric.INNER_PRODUCT:
+            want, tol = -dot, 1e-5 * mag + 1e-7
+        elif metric == Metric.COSINE_NORMALIZED:
+            want, tol = 1 - dot, 1e-5 * mag + 1e-6
+        else:
+            want = 1 - np.clip(dot / np.sqrt(qq * xx), -1, 1)
+            tol = np.full(want.shape, 1e-5)
+        err = np.abs(got - want)
+        assert (err <= tol).all(), (kind, float((err / tol).max()))

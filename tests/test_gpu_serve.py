@@ -179,3 +179,85 @@ def test_replay_far_above_capacity_returns_each_request_its_own_results():
     wrong = np.flatnonzero((ids[:, :10] != exp_ids).any(1))
     assert wrong.size == 0, f"{wrong.size} of {m} requests got other results, first {wrong[:5]}"
     np.testing.assert_array_equal(dists[:, :10].view(np.uint32), exp_d.view(np.uint32))
+
+
+def _oracle_check(orc, q, k, l, res):
+    ids, dists, st = res
+    oi, od, os_ = orc.search(q[None, :], k, l, 1, O.STRATEGY_FULL_PRECISION)
+    np.testing.assert_array_equal(ids, oi[0])
+    np.testing.assert_array_equal(dists.view(np.uint32), od[0].view(np.uint32))
+    assert st["cmps"] == os_["cmps"][0] and st["hops"] == os_["hops"][0]
+
+
+def test_cancelled_requests_and_the_server_stays_usable():
+    """dk_server_cancel: a cancelled request (whether still queued or already on the device)
+    polls as CANCELLED and frees its slot and memory; the others complete exactly; cancelling
+    a collected ticket is NOT_FOUND; the server serves new requests afterwards."""
+    v, a, d, n = random_index(20000, 64, 32, seed=21)
+    q = queries_like(v[:n], 64, seed=22)
+    orc = O.OracleIndex(v, a, d, n, O.METRIC_L2)
+    prov = GpuProvider(v, a, d, n, Metric.L2)
+    # One launch context: while the first launch runs, later submits wait in the queue.
+    srv = SearchServer(prov, FullPrecision(), max_k=10, max_l=400, queue_depth=64, streams=1)
+    tickets = [srv.submit(q[i], 10, 400) for i in range(len(q))]
+    cancelled = set(tickets[1::3])
+    for t in cancelled:
+        srv.cancel(t)
+        srv.cancel(t)  # cancelling twice is harmless
+    for i, t in enumerate(tickets):
+        if t in cancelled:
+            with pytest.raises(ANNError) as ei:
+                srv.wait(t, 10)
+            assert ei.value.status == Status.CANCELLED
+        else:
+            _oracle_check(orc, q[i], 10, 400, srv.wait(t, 10))
+    with pytest.raises(ANNError) as ei:
+        srv.cancel(tickets[0])
+    assert ei.value.status == Status.NOT_FOUND
+    assert srv.info()["reserved_bytes"] == 0
+    _oracle_check(orc, q[5], 10, 100, srv.wait(srv.submit(q[5], 10, 100), 10))
+    srv.close()
+
+
+def test_admission_by_beam_state_memory_and_by_queue_depth():
+    """A request is admitted while the device memory its beam state needs at its own L fits
+    beside the outstanding requests' reservations: with a budget for a few requests, the next
+    submit is rejected with ADMISSION (a host-side failure, nothing reaches the device), a
+    larger L takes more of the budget, and collecting a request makes room again.  A full
+    queue (queue_depth outstanding) is rejected the same way."""
+    v, a, d, n = random_index(5000, 32, 24, seed=31)
+    q = queries_like(v[:n], 16, seed=32)
+    orc = O.OracleIndex(v, a, d, n, O.METRIC_L2)
+    prov = GpuProvider(v, a, d, n, Metric.L2)
+    probe = SearchServer(prov, FullPrecision(), max_k=10, max_l=512, queue_depth=64)
+    t = probe.submit(q[0], 10, 64)
+    small = probe.info()["reserved_bytes"]
+    probe.wait(t, 10)
+    t = probe.submit(q[0], 10, 512)
+    large = probe.info()["reserved_bytes"]
+    probe.wait(t, 10)
+    probe.close()
+    assert large > 4 * small > 0
+    srv = SearchServer(prov, FullPrecision(), max_k=10, max_l=512, queue_depth=64,
+                       memory_bytes=3 * small + small // 2)
+    held = [srv.submit(q[i], 10, 64) for i in range(3)]
+    with pytest.raises(ANNError) as ei:
+        srv.submit(q[3], 10, 64)
+    assert ei.value.status == Status.ADMISSION and "memory" in str(ei.value)
+    with pytest.raises(ANNError) as ei:
+        srv.submit(q[3], 10, 512)  # never fits this budget
+    assert ei.value.status == Status.ADMISSION
+    _oracle_check(orc, q[0], 10, 64, srv.wait(held[0], 10))
+    t = srv.submit(q[3], 10, 64)  # room again
+    for i, tk in zip((1, 2, 3), held[1:] + [t]):
+        _oracle_check(orc, q[i], 10, 64, srv.wait(tk, 10))
+    assert srv.info()["reserved_bytes"] == 0
+    srv.close()
+    full = SearchServer(prov, FullPrecision(), max_k=10, max_l=64, queue_depth=2)
+    t0, t1 = full.submit(q[0], 10, 64), full.submit(q[1], 10, 64)
+    with pytest.raises(ANNError) as ei:
+        full.submit(q[2], 10, 64)
+    assert ei.value.status == Status.ADMISSION and "queue_depth" in str(ei.value)
+    full.wait(t0, 10)
+    full.wait(t1, 10)
+    full.close()
