@@ -1426,36 +1426,55 @@ __device__ __forceinline__ uint32_t warp_next_cursor(uint32_t cap, const State& 
   return nc;
 }
 
-// Write the merged queue into the other buffer (see the file comment for the order rule).
-// Entries before the first insertion point p0 keep their positions; only the rest are ranked.
+// Merge the ordered new items into the queue in place (see the file comment for the order
+// rule).  Entries before the first insertion point p0 stay where they are; each later entry
+// moves right by the number of new items at or below its distance (a new item goes before
+// old items of equal distance), handled 32 at a time from the back, so every entry is read
+// before anything is written over it (the destinations keep their order); entries pushed past
+// the capacity drop.  The new items' final positions are taken first, from the queue as it
+// was.  Before this in-place form every hop rewrote the whole queue into a second buffer; at
+// L = 512 that copy was the largest part of a hop.
 __device__ __forceinline__ void warp_commit_merge(uint32_t cap, const State& S,
                                                   uint32_t nvalid, uint32_t nc, uint32_t lane,
                                                   uint32_t& size, uint32_t& cursor,
                                                   uint32_t& cur) {
-  const uint32_t nxt = cur ^ 1u;
   const uint32_t new_size = min(size + nvalid, cap);
-  const float* od = S.qd[cur];
-  const uint32_t* oi = S.qi[cur];
-  float* wd = S.qd[nxt];
-  uint32_t* wi = S.qi[nxt];
-  const uint32_t p0 = nvalid ? count_less(od, size, S.new_d[0]) : size;
-  for (uint32_t o = lane; o < p0; o += 32u) {
-    wd[o] = od[o];
-    wi[o] = oi[o];
-  }
-  for (uint32_t o = p0 + lane; o < size; o += 32u) {
-    const float d = od[o];
-    const uint32_t pos = o + count_less_equal(S.new_d, nvalid, d);
-    if (pos < cap) { wd[pos] = d; wi[pos] = oi[o]; }
-  }
-  for (uint32_t r = lane; r < nvalid; r += 32u) {
-    const float d = S.new_d[r];
-    const uint32_t pos = r + p0 + count_less(od + p0, size - p0, d);
-    if (pos < cap) { wd[pos] = d; wi[pos] = S.new_id[r]; }
+  float* qd = S.qd[cur];
+  uint32_t* qi = S.qi[cur];
+  if (nvalid > 0u) {
+    const uint32_t p0 = count_less(qd, size, S.new_d[0]);
+    // The hop's candidate list is consumed: it holds the new items' final positions.
+    for (uint32_t r = lane; r < nvalid; r += 32u)
+      S.cand_id[r] = r + p0 + count_less(qd + p0, size - p0, S.new_d[r]);
+    __syncwarp();
+    for (int32_t c0 = (int32_t)size - 32; c0 + 32 > (int32_t)p0; c0 -= 32) {
+      const int32_t o = c0 + (int32_t)lane;
+      const bool live = o >= (int32_t)p0 && o < (int32_t)size;
+      float d = 0.0f;
+      uint32_t id = 0u, pos = cap;
+      if (live) {
+        d = qd[o];
+        id = qi[o];
+        pos = (uint32_t)o + count_less_equal(S.new_d, nvalid, d);
+      }
+      __syncwarp();
+      if (live && pos < cap) {
+        qd[pos] = d;
+        qi[pos] = id;
+      }
+      __syncwarp();
+    }
+    for (uint32_t r = lane; r < nvalid; r += 32u) {
+      const uint32_t pos = S.cand_id[r];
+      if (pos < cap) {
+        qd[pos] = S.new_d[r];
+        qi[pos] = S.new_id[r];
+      }
+    }
   }
   cursor = nc;
   size = new_size;
-  cur = nxt;
+  (void)cur;  // the queue stays in buffer `cur`; the other buffer is the rerank's scratch
   __syncwarp();
 }
 
