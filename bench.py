@@ -52,7 +52,7 @@ WORKLOADS = {
     # L2-normalised, inner product.
     "ip768": dict(n=1_000_000, dim=768, normalized=True, metric=1, comps=0, sigma=0.0,
                   nq=10_000, R=64, l_build=128, alpha=1.2, pq_chunks=0, pq_train=0, k=10,
-                  l_sweep=[128, 192, 256], strategies=["fp32", "bf16", "fp8"],
+                  l_sweep=[128, 192, 256, 512, 1024, 2048], strategies=["fp32", "bf16", "fp8"],
                   seed=0xD15CA77 + 3),
     # The same rows under CosineNormalized (1 - dot: the inner-product ranking on normalised
     # rows, with the triangle-inequality prune instead of the occluding one).
@@ -66,7 +66,7 @@ WORKLOADS = {
     "ip20m": dict(n=20_000_000, dim=384, normalized=True, metric=1, comps=1024, sigma=8.0,
                   mean_range=(-50.0, 50.0), clip=(-255.0, 255.0),
                   nq=10_000, R=32, l_build=200, alpha=1.2, pq_chunks=48, pq_train=100_000, k=10,
-                  l_sweep=[64, 100, 128, 192, 256, 384, 512, 768],
+                  l_sweep=[64, 100, 128, 192, 256, 384, 512, 576, 640, 768],
                   strategies=["fp32", "bf16", "fp8", "hybrid"], seed=0xD15CA77 + 5, cache=False,
                   gt_queries=1000, gt_prefilter=256),
     # The large FP8 served shape exactly as specified: 20M x 384 isotropic Gaussian rows scaled
@@ -540,9 +540,10 @@ def run_ours(args, data, rank, world):
     e2e_s = max_over_ranks(float(np.mean(e2e_t)) * 1e3, world) / 1e3
 
     # Serving (N=1 only): per strategy, Poisson arrivals replayed through dk_server_* at
-    # offered rates doubling from 250k requests/s until the server saturates (achieved below
-    # 90 % of offered, or p99 above SERVE_P99_BOUND_MS); capacity = the highest achieved rate
-    # whose p99 stays within the bound.  Plus the mixed-k/L stream at 100k requests/s.
+    # offered rates doubling from a quarter of the strategy's batch QPS until the server
+    # saturates (achieved below 90 % of offered, or p99 above SERVE_P99_BOUND_MS); capacity =
+    # the highest achieved rate whose p99 stays within the bound.  Plus the mixed-k/L stream at
+    # 100k requests/s (or the batch QPS / 10 when that is lower).
     serving = None
     if world == 1 and not args.no_serving:
         serving = {}
@@ -551,7 +552,7 @@ def run_ours(args, data, rank, world):
                 continue
             st_obj, ls = strategies[name], table[name]["L"]
             rows, cap = [], 0.0
-            rate = 250_000.0
+            rate = float(max(1000, int(table[name]["qps"] / 4 / 1000) * 1000))
             while rate <= 8_000_000.0:
                 secs = min(args.serve_seconds, 2_000_000.0 / rate)
                 row = serve_latency(provider, st_obj, queries, gt, k, ls, rate, secs)
@@ -562,7 +563,8 @@ def run_ours(args, data, rank, world):
                 if not ok or row["achieved_qps"] < 0.9 * rate:
                     break
                 rate *= 2.0
-            mixed = serve_latency(provider, st_obj, queries, gt, k, ls, 100_000.0,
+            mixed = serve_latency(provider, st_obj, queries, gt, k, ls,
+                                  min(100_000.0, float(int(table[name]["qps"] / 10))),
                                   args.serve_seconds, mixed=True)
             serving[name] = {"L": ls, "p99_bound_ms": SERVE_P99_BOUND_MS,
                              "capacity_qps": round(cap, 1), "rates": rows, "mixed": mixed}

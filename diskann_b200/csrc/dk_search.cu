@@ -138,12 +138,17 @@ int32_t plan_warp(dk_index* ix, SearchParams& P, LaunchPlan& L, int mode, double
   // Per-warp budget (measured on the 1M x 128 and 2M x 384 workloads): the kernels are fastest
   // with a shared level holding ~1.1x the mean visited set at load 3/4 (12-32 KB per warp),
   // which keeps nearly every probe out of the global level, rather than with more resident
-  // warps (2M x 384 at L = 512: 342k QPS with 20 KB per warp, 371k with 28 KB).  PQ
+  // warps (2M x 384 at L = 512: 342k QPS with 20 KB per warp, 371k with 28 KB); beyond 32 KB
+  // see below.  PQ
   // traversal keeps its ADC table and a minimal level.  DK_WARP_SMEM overrides.
   uint32_t dflt = 12288;
   if (mode != kModePQ) {
     dflt = base + (uint32_t)(4.0 * est_mean * 1.1 / 0.75);
-    dflt = std::min<uint32_t>(std::max<uint32_t>(dflt, 12288), 32768);
+    // A visited set too large for a 32 KB slice goes mostly to the global level whatever the
+    // slice, and then more resident warps pay more than a larger shared level: 20M x 384 at
+    // L = 512 (8.4k visited ids) ran 185k QPS with 24 KB per warp, 150k with 32 KB, 131k with
+    // 48 KB.
+    dflt = dflt > 32768 ? 24576 : std::max<uint32_t>(dflt, 12288);
   }
   const uint32_t budget = std::max<uint32_t>(env_u32("DK_WARP_SMEM", dflt), base + 1024);
   uint32_t slots = align_up((uint32_t)(est_mean * 1.3 / 0.75) + 1, 32);

@@ -17,12 +17,13 @@ def knn_f64(base: np.ndarray, queries: np.ndarray, k: int, metric: int = 2,
     """Return ``(ids uint32 (nq, k), dists float64 (nq, k))`` of the exact k nearest rows.
 
     ``prefilter`` = C > 0 (for bases too large to scan in float64, e.g. 20M x 384): each
-    query's C best rows by a BF16 tensor-core score are taken first, then ranked by their exact
-    float64 distances.  The k nearest are among the C as long as BF16 rounding (about 2^-9 of
-    each product) cannot move a true neighbour below the C-th candidate; with C = 256 and k = 10
-    the margin between the 10th and the 256th best score is far above that rounding on the
-    benchmark shapes, and tests/test_gpu_groundtruth.py checks the result equals the full
-    float64 scan."""
+    query's C best rows by a lower-precision score are taken first, then ranked by their exact
+    float64 distances.  The score is a BF16 tensor-core dot product for the angular metrics
+    (unit-scale rows) and an FP32 one for L2, whose |x|^2 - 2 q.x on unnormalised rows loses
+    too much in BF16.  The k nearest are among the C as long as that rounding cannot move a
+    true neighbour below the C-th candidate; with C = 256 and k = 10 the margin between the 10th
+    and the 256th best score is far above it on the benchmark shapes, and
+    tests/test_gpu_groundtruth.py checks the result equals the full float64 scan."""
     if prefilter:
         return _knn_prefiltered(base, queries, k, metric, device, base_chunk, query_block,
                                 prefilter)
@@ -92,13 +93,14 @@ def _knn_prefiltered(base, queries, k, metric, device, base_chunk, query_block, 
     cand = min(cand, n)
     out_i = np.empty((Q.shape[0], k), np.uint32)
     out_d = np.empty((Q.shape[0], k), np.float64)
+    low = torch.float32 if metric == 2 else torch.bfloat16
     for q0 in range(0, Q.shape[0], query_block):
         q = Q[q0:q0 + query_block]
-        qb = q.to(torch.bfloat16)
+        qb = q.to(low)
         best_s = best_i = None
         for b0 in range(0, n, base_chunk):
             x = B[b0:b0 + base_chunk]
-            dot = (qb @ x.to(torch.bfloat16).T).float()
+            dot = (qb @ x.to(low).T).float()
             if metric == 2:  # smaller |x|^2 - 2 q.x is nearer
                 score = (x.float() * x.float()).sum(1)[None, :] - 2.0 * dot
             elif metric == 0:
