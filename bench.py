@@ -2,9 +2,10 @@
 
 Default workload (``pq1m``): 1M x 128 float32 seeded Gaussian mixture (256 components,
 sigma 8, means U[0,100], clipped to [0,255]); PQ 32 x 256 trained on a 100k sample; Vamana
-R=64, L_build=100, alpha=1.2 (slot width 83); 10,000 queries from the same mixture; k=10;
-Hybrid strategy (ADC traversal, exact FP32 L2 rerank of the top L); L is the smallest of
-50/75/100/150/200 whose recall@10 against float64 ground truth is >= 0.95.
+R=64, L_build=100, alpha=1.2 (slot width 83); 10,000 queries from the same mixture; k=10.
+Every strategy (FP32, BF16, FP8, Hybrid) is timed at the smallest L of its sweep whose
+recall@10 against float64 ground truth reaches 0.95; the headline is the plain FP32 path (the
+strategy whose results equal the reference's search), the others are reported beside it.
 
 A step = one batched search of all queries.  ``value`` times the search with queries and
 outputs resident in HBM (CUDA events on the launching stream, L2 flushed before every step);
@@ -12,7 +13,8 @@ outputs resident in HBM (CUDA events on the launching stream, L2 flushed before 
 copy of the queries, search, device->host copy of ids, distances and stats).
 
 ``--impl reference`` times the CPU restatement of the reference search (the oracle, all host
-threads) on the same workload, metric and L.
+threads) on the same workload, metric and L, on a graph the oracle builds itself (the same
+graph; that process loads none of this library).
 
 Multi-GPU (``torchrun --nproc-per-node N``): replicas — each rank holds the whole index and
 searches its own copy of the query batch; ``value`` = all ranks' queries / max-over-ranks time.
@@ -487,9 +489,12 @@ def run_ours(args, data, rank, world):
         row["qps"] = round(timed(Knn(k, row["L"]), strat), 1)
         table[name] = row
         log(f"[ours] {name}: {row}")
+    # Headline: the plain FP32 path (the strategy whose results equal the reference's search,
+    # and the one the CPU reference arm runs) when it reaches the recall target; the precision
+    # forms are reported beside it as QPS ratios.  Otherwise the fastest strategy that does.
     reached = {n: r for n, r in table.items() if r["reached"]}
     pool = reached or table
-    head = max(pool, key=lambda n: pool[n]["qps"])
+    head = "fp32" if "fp32" in reached else max(pool, key=lambda n: pool[n]["qps"])
     chosen = table[head]["L"]
     strategy = strategies[head]
     params = Knn(k, chosen)
@@ -540,7 +545,7 @@ def run_ours(args, data, rank, world):
     e2e_s = max_over_ranks(float(np.mean(e2e_t)) * 1e3, world) / 1e3
 
     # Serving (N=1 only): per strategy, Poisson arrivals replayed through dk_server_* at
-    # offered rates doubling from a quarter of the strategy's batch QPS until the server
+    # offered rates growing 1.5x from a quarter of the strategy's batch QPS until the server
     # saturates (achieved below 90 % of offered, or p99 above SERVE_P99_BOUND_MS); capacity =
     # the highest achieved rate whose p99 stays within the bound.  Plus the mixed-k/L stream at
     # 100k requests/s (or the batch QPS / 10 when that is lower).
@@ -562,7 +567,7 @@ def run_ours(args, data, rank, world):
                     cap = max(cap, row["achieved_qps"])
                 if not ok or row["achieved_qps"] < 0.9 * rate:
                     break
-                rate *= 2.0
+                rate = float(int(rate * 1.5 / 1000) * 1000)
             mixed = serve_latency(provider, st_obj, queries, gt, k, ls,
                                   min(100_000.0, float(int(table[name]["qps"] / 10))),
                                   args.serve_seconds, mixed=True)
