@@ -463,13 +463,16 @@ def run_ours(args, data, rank, world):
             continue
         strat = strategies[name]
         row = None
+        sweep = []
         for l in w["l_sweep"]:
             search(Knn(k, l), strat)
             torch.cuda.synchronize()
             r = recall_at_k(ids.cpu().numpy().view(np.uint32), gt, k)
+            sweep.append({"L": l, "recall": round(r, 4), "qps": round(timed(Knn(k, l), strat, 1), 1)})
             row = {"L": l, "recall": round(r, 4), "reached": r >= TARGET_RECALL}
             if r >= TARGET_RECALL:
                 break
+        row["sweep"] = sweep
         search(Knn(k, row["L"]), strat)
         torch.cuda.synchronize()
         err = max_rel_dist_error(ids.cpu().numpy().view(np.uint32), dists.cpu().numpy(), data,
