@@ -139,10 +139,14 @@ int32_t plan_warp(dk_index* ix, SearchParams& P, LaunchPlan& L, int mode, double
   // with a shared level holding ~1.1x the mean visited set at load 3/4 (12-32 KB per warp),
   // which keeps nearly every probe out of the global level, rather than with more resident
   // warps (2M x 384 at L = 512: 342k QPS with 20 KB per warp, 371k with 28 KB); beyond 32 KB
-  // see below.  PQ
-  // traversal keeps its ADC table and a minimal level.  DK_WARP_SMEM overrides.
+  // see below.  PQ traversal keeps its 32 KB-class ADC table beside a level sized the same
+  // way, up to 96 KB per warp: with a 1 KB level the 1M x 128 Hybrid search at L = 400 sent
+  // nearly every probe to the global level (4.8 GB of DRAM writes per launch) and ran 145k QPS;
+  // with a 74 KB slice, 186k.  DK_WARP_SMEM overrides.
   uint32_t dflt = 12288;
-  if (mode != kModePQ) {
+  if (mode == kModePQ) {
+    dflt = std::min<uint32_t>(base + (uint32_t)(4.0 * est_mean * 1.1 / 0.75), 98304);
+  } else {
     dflt = base + (uint32_t)(4.0 * est_mean * 1.1 / 0.75);
     // A visited set too large for a 32 KB slice goes mostly to the global level whatever the
     // slice, and then more resident warps pay more than a larger shared level: 20M x 384 at
