@@ -332,21 +332,27 @@ __device__ __forceinline__ void subgroup_distances(const RowT* const (&rows)[U],
   float acc[U][4];
 #pragma unroll
   for (int u = 0; u < U; ++u) acc[u][0] = acc[u][1] = acc[u][2] = acc[u][3] = 0.0f;
-  if (DIM > 0 && DIM % 32 == 0 && DIM / 32 * U <= 16) {
-    // Every 16-byte piece of the U rows is requested before the first FMA, so one round
-    // costs one memory latency.  The FMAs then run in the reference's block order.
+  if (DIM > 0 && DIM % 32 == 0) {
+    // The 16-byte pieces of the U rows are requested CH blocks at a time (at most 16 pieces
+    // per lane in flight) before their FMAs, so a row of up to 16·32 floats costs one memory
+    // latency and a 768-float row two.  The FMAs run in the reference's block order.
     constexpr int NB = DIM > 0 ? DIM / 32 : 1;
-    float4 v[U][NB];
+    constexpr int CH = (16 / U) < NB ? (16 / U) : NB;
 #pragma unroll
-    for (int u = 0; u < U; ++u)
+    for (int c0 = 0; c0 < NB; c0 += CH) {
+      float4 v[U][CH];
 #pragma unroll
-      for (int b = 0; b < NB; ++b)
-        v[u][b] = ld4(rows[u], 8 * b + s);
+      for (int u = 0; u < U; ++u)
 #pragma unroll
-    for (int b = 0; b < NB; ++b) {
-      const float4 a = q4[8 * b + s];
+        for (int j = 0; j < CH; ++j)
+          if (c0 + j < NB) v[u][j] = ld4(rows[u], 8 * (c0 + j) + s);
 #pragma unroll
-      for (int u = 0; u < U; ++u) acc4<METRIC>(a, v[u][b], acc[u]);
+      for (int j = 0; j < CH; ++j) {
+        if (c0 + j >= NB) break;
+        const float4 a = q4[8 * (c0 + j) + s];
+#pragma unroll
+        for (int u = 0; u < U; ++u) acc4<METRIC>(a, v[u][j], acc[u]);
+      }
     }
   } else {
 #pragma unroll 4
@@ -748,6 +754,18 @@ __device__ __forceinline__ void score_lp_wide(const SearchParams& P, const float
   const float qq = (METRIC == DK_METRIC_L2 || METRIC == DK_METRIC_COSINE)
                        ? subgroup_qq<kPer>(q, Sh::kPieces, s, gmask) : 0.0f;
   const uint32_t step = nsub * U;
+  if constexpr (U == 1) {
+    // Wide rows (one per subgroup per round): the rows of the later rounds are requested into
+    // L2 first, as the FP32 scorer does for its wide rows.
+    if (count > step) {
+      const uint32_t lines = (row_bytes + 127u) / 128u;
+      const uint32_t total = (count - step) * lines;
+      for (uint32_t e = sg * 8u + s; e < total; e += nsub * 8u) {
+        const unsigned char* r = base + (size_t)ids[step + e / lines] * row_bytes + (e % lines) * 128u;
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(r));
+      }
+    }
+  }
   for (uint32_t b0 = 0; b0 < count; b0 += step) {
     uint32_t idx[U], rid[U];
     uint4 w[U][NP];
