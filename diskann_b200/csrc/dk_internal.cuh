@@ -92,6 +92,9 @@ struct SearchParams {
   uint32_t* gtable;
   uint32_t gtable_log2;
   uint32_t gtable_limit;
+  // Warp kernel: issue a whole adjacency row's global-level probes together (one round trip
+  // per row; the default) instead of one round trip per 32-id round.
+  uint32_t row_probes;
   // Shared-memory carve-up: byte offsets from the CTA's dynamic shared memory (CTA kernel)
   // or from the warp's slice of it (warp kernel, slices of `warp_smem` bytes).
   uint32_t off_query, off_table, off_qd0, off_qi0, off_qd1, off_qi1;

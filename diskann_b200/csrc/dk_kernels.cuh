@@ -1685,9 +1685,9 @@ __device__ __forceinline__ void warp_query(const SearchParams& P, const State& S
           ids[r] = t < P.max_degree ? __ldg(row + 1 + t) : 0u;
         }
       }
-      // Low-precision traversal: a row's global-level probes go out together.  The FP32 path
-      // keeps one round at a time, which measured faster with its register-heavier scoring.
-      if ((MODE == kModeBF16 || MODE == kModeFP8) && deg <= 128u) {
+      // A row's global-level probes go out together (one round trip per row): always for the
+      // low-precision traversal, and for the other modes unless P.row_probes is cleared.
+      if ((MODE == kModeBF16 || MODE == kModeFP8 || P.row_probes) && deg <= 128u) {
         bool fresh[4];
         vset.insert_row(ids, deg, lane, fresh);
 #pragma unroll

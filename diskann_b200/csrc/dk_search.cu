@@ -150,9 +150,9 @@ int32_t plan_warp(dk_index* ix, SearchParams& P, LaunchPlan& L, int mode, double
     dflt = base + (uint32_t)(4.0 * est_mean * 1.1 / 0.75);
     // A visited set too large for a 32 KB slice goes mostly to the global level whatever the
     // slice, and then more resident warps pay more than a larger shared level: 20M x 384 at
-    // L = 512 (8.4k visited ids) ran 185k QPS with 24 KB per warp, 150k with 32 KB, 131k with
-    // 48 KB.
-    dflt = dflt > 32768 ? 24576 : std::max<uint32_t>(dflt, 12288);
+    // L = 512 (8.4k visited ids) ran 150k QPS with 32 KB per warp, 131k with 48 KB, 185k with
+    // 24 KB, 233k with 16 KB and 245k with 14 KB (16 warps per SM, the register limit).
+    dflt = dflt > 32768 ? 14336 : std::max<uint32_t>(dflt, 12288);
   }
   const uint32_t budget = std::max<uint32_t>(env_u32("DK_WARP_SMEM", dflt), base + 1024);
   uint32_t slots = align_up((uint32_t)(est_mean * 1.3 / 0.75) + 1, 32);
@@ -161,6 +161,10 @@ int32_t plan_warp(dk_index* ix, SearchParams& P, LaunchPlan& L, int mode, double
   slots = std::max<uint32_t>(slots, 64);
   P.hash_slots = slots;
   P.hash_limit = slots * 3 / 4;
+  // One global round trip per adjacency row for every mode: measured faster than one per
+  // 32-id round for FP32 too (1M x 128 L = 50 +2.3 %, 2M x 384 L = 512 +4 %, 20M x 384
+  // L = 512 +6.6 %).  DK_ROW_PROBES=0 restores one round trip per round.
+  P.row_probes = env_u32("DK_ROW_PROBES", 1u) ? 1u : 0u;
   P.hash_log2 = log2_at_least(slots, 6, 16);  // only sizes the shared-memory carve-up below
   P.warp_smem = base + align_up(slots * 4, 16);
   plan_query_smem(P, pq, false);
