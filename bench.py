@@ -549,8 +549,9 @@ def run_ours(args, data, rank, world):
 
     # Serving (N=1 only): per strategy, Poisson arrivals replayed through dk_server_* at
     # offered rates growing 1.5x from a quarter of the strategy's batch QPS until the server
-    # saturates (achieved below 90 % of offered, or p99 above SERVE_P99_BOUND_MS); capacity =
-    # the highest achieved rate whose p99 stays within the bound.  Plus the mixed-k/L stream at
+    # saturates (achieved below 90 % of offered, or p99 above the bound: SERVE_P99_BOUND_MS, or
+    # twice the p99 at the lightest load when a single search takes longer); capacity = the
+    # highest achieved rate whose p99 stays within the bound.  Plus the mixed-k/L stream at
     # 100k requests/s (or the batch QPS / 10 when that is lower).
     serving = None
     if world == 1 and not args.no_serving:
@@ -561,11 +562,14 @@ def run_ours(args, data, rank, world):
             st_obj, ls = strategies[name], table[name]["L"]
             rows, cap = [], 0.0
             rate = float(max(1000, int(table[name]["qps"] / 4 / 1000) * 1000))
+            bound = SERVE_P99_BOUND_MS
             while rate <= 8_000_000.0:
                 secs = min(args.serve_seconds, 2_000_000.0 / rate)
                 row = serve_latency(provider, st_obj, queries, gt, k, ls, rate, secs)
                 rows.append(row)
-                ok = row["p99_ms"] <= SERVE_P99_BOUND_MS
+                if len(rows) == 1:  # long searches: twice the p99 of the lightest load
+                    bound = max(SERVE_P99_BOUND_MS, 2.0 * row["p99_ms"])
+                ok = row["p99_ms"] <= bound
                 if ok:
                     cap = max(cap, row["achieved_qps"])
                 if not ok or row["achieved_qps"] < 0.9 * rate:
@@ -574,10 +578,10 @@ def run_ours(args, data, rank, world):
             mixed = serve_latency(provider, st_obj, queries, gt, k, ls,
                                   min(100_000.0, float(int(table[name]["qps"] / 10))),
                                   args.serve_seconds, mixed=True)
-            serving[name] = {"L": ls, "p99_bound_ms": SERVE_P99_BOUND_MS,
+            serving[name] = {"L": ls, "p99_bound_ms": round(bound, 3),
                              "capacity_qps": round(cap, 1), "rates": rows, "mixed": mixed}
             log(f"[ours] serving {name}: capacity {cap:.0f} req/s at p99 <= "
-                f"{SERVE_P99_BOUND_MS} ms; {rows} mixed {mixed}")
+                f"{bound:.3f} ms; {rows} mixed {mixed}")
 
     mean_deg = float(data["deg"][: data["n"]].mean())
     alg = algorithmic_bytes(stats_np, w, chosen, mean_deg, head)
