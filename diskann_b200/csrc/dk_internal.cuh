@@ -99,6 +99,9 @@ struct SearchParams {
   // or from the warp's slice of it (warp kernel, slices of `warp_smem` bytes).
   uint32_t off_query, off_table, off_qd0, off_qi0, off_qd1, off_qi1;
   uint32_t off_cand_id, off_cand_d, off_new_d, off_new_id, off_hash, off_misc;
+  // Warp kernel, strategies without a rerank: the queue is merged in place and its second
+  // buffer (the rerank's scratch) is not needed, so both queue buffers alias one region.
+  uint32_t single_queue;
   uint32_t smem_bytes;
   uint32_t warp_smem;
   uint32_t list_cap;  // capacity of the candidate / rerank lists

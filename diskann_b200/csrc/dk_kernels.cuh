@@ -1749,7 +1749,9 @@ template <int METRIC, int MODE, int DIM, int U>
 // blocks caps them at 128 registers (FP32 at D = 128 with four rows per subgroup spills 12
 // bytes; no other variant spills), measured 2 % (FP32) and 5-9 % (BF16 / FP8) faster on a
 // 1M-point graph than with the ~160-170 registers of a one-block minimum.  PQ keeps the
-// one-block minimum (up to 255 registers).
+// one-block minimum (up to 255 registers).  (A six-block minimum for rows wider than 128
+// elements, 85 registers, let 24 warps stay resident on long searches but measured 5-8 % slower
+// on 2M x 384 and 11 % slower for BF16 on 20M x 384, for 1 % on FP32 there.)
 __global__ void __launch_bounds__(128, (MODE == kModePQ) ? 1 : 4)
     k_search_warp(const SearchParams P) {
   extern __shared__ __align__(16) unsigned char smem[];

@@ -170,6 +170,7 @@ extern "C" int32_t dk_search_device_noalloc(dk_index* ix, int32_t strategy, cons
     spill_ctas = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(spill_ctas, (cap_bytes - 256) / per_bitmap));
   }
   SearchParams P2 = P;
+  P2.single_queue = 0;  // the spill pass (CTA kernel) merges into its second queue buffer
   P2.hash_limit = 0xFFFFFFFFu;  // the bitmap never fills
   P2.smem_bytes = dk::plan_query_smem(P2, pq, false);
   if (P2.smem_bytes > (uint32_t)max_optin) return too_big_smem();

@@ -49,8 +49,8 @@ uint32_t plan_query_smem(SearchParams& P, bool pq, bool with_hash) {
   P.off_table = take(pq ? P.pq_chunks * 256u * 4u : 0u);
   P.off_qd0 = take(P.cap * 4);
   P.off_qi0 = take(P.cap * 4);
-  P.off_qd1 = take(P.cap * 4);
-  P.off_qi1 = take(P.cap * 4);
+  P.off_qd1 = P.single_queue ? P.off_qd0 : take(P.cap * 4);
+  P.off_qi1 = P.single_queue ? P.off_qi0 : take(P.cap * 4);
   P.off_cand_id = take(P.list_cap * 4);
   P.off_cand_d = take(P.list_cap * 4);
   P.off_new_d = take(P.list_cap * 4);
@@ -134,6 +134,7 @@ int32_t plan_warp(dk_index* ix, SearchParams& P, LaunchPlan& L, int mode, double
   // Shared level: room for 1.3x the mean visited set at <= 3/4 load, within a per-warp
   // shared-memory budget; the global level takes what a longer search adds.
   P.hash_log2 = 0;
+  P.single_queue = strategy_reranks(P.strategy) ? 0u : 1u;
   const uint32_t base = plan_query_smem(P, pq, false);
   // Per-warp budget (measured on the 1M x 128 and 2M x 384 workloads): the kernels are fastest
   // with a shared level holding ~1.1x the mean visited set at load 3/4 (12-32 KB per warp),
@@ -151,8 +152,9 @@ int32_t plan_warp(dk_index* ix, SearchParams& P, LaunchPlan& L, int mode, double
     // A visited set too large for a 32 KB slice goes mostly to the global level whatever the
     // slice, and then more resident warps pay more than a larger shared level: 20M x 384 at
     // L = 512 (8.4k visited ids) ran 150k QPS with 32 KB per warp, 131k with 48 KB, 185k with
-    // 24 KB, 233k with 16 KB and 245k with 14 KB (16 warps per SM, the register limit).
-    dflt = dflt > 32768 ? 14336 : std::max<uint32_t>(dflt, 12288);
+    // 24 KB, 233k with 16 KB and 245k with 14 KB (16 warps per SM, the register limit at 128
+    // registers).
+    dflt = dflt > 32768 ? std::max<uint32_t>(14336, base + 2048) : std::max<uint32_t>(dflt, 12288);
   }
   const uint32_t budget = std::max<uint32_t>(env_u32("DK_WARP_SMEM", dflt), base + 1024);
   uint32_t slots = align_up((uint32_t)(est_mean * 1.3 / 0.75) + 1, 32);
@@ -268,6 +270,7 @@ int32_t dk_launch_search(dk_index* ix, int32_t strategy, const float* queries,
   }
 
   SearchParams P2 = P;
+  P2.single_queue = 0;  // the spill pass (CTA kernel) merges into its second queue buffer
   P2.hash_limit = 0xFFFFFFFFu;  // the bitmap never fills
   P2.smem_bytes = dk::plan_query_smem(P2, pq, false);
   if (P2.smem_bytes > (uint32_t)max_optin) return too_big();
