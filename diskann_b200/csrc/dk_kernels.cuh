@@ -1542,10 +1542,11 @@ __device__ void warp_post_process(const SearchParams& P, const State& S, const Q
                                   uint32_t& result_count) {
   const float* qd = S.qd[cur];
   const uint32_t* qi = S.qi[cur];
-  // The rerank list (up to L + F entries) lives in the queue's other buffer, free after the
-  // last merge.
-  uint32_t* rid = S.qi[cur ^ 1u];
-  float* rd = S.qd[cur ^ 1u];
+  // The rerank list (up to L + F ids and distances) lives in the shared visited level when the
+  // queue has one buffer (the planner sizes the level for it; every query clears the level
+  // before its search), else in the queue's other buffer, free after the last merge.
+  uint32_t* rid = P.single_queue ? S.hash : S.qi[cur ^ 1u];
+  float* rd = P.single_queue ? reinterpret_cast<float*>(S.hash + P.cap) : S.qd[cur ^ 1u];
   uint32_t* out_ids = io.ids;
   float* out_d = io.dists;
   const uint32_t k = io.k;

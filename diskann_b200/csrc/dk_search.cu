@@ -134,7 +134,9 @@ int32_t plan_warp(dk_index* ix, SearchParams& P, LaunchPlan& L, int mode, double
   // Shared level: room for 1.3x the mean visited set at <= 3/4 load, within a per-warp
   // shared-memory budget; the global level takes what a longer search adds.
   P.hash_log2 = 0;
-  P.single_queue = strategy_reranks(P.strategy) ? 0u : 1u;
+  // One queue buffer: the merge works in place, and a rerank's list (up to L + F ids and
+  // distances) goes into the shared visited level, which the search no longer needs by then.
+  P.single_queue = 1u;
   const uint32_t base = plan_query_smem(P, pq, false);
   // Per-warp budget (measured on the 1M x 128 and 2M x 384 workloads): the kernels are fastest
   // with a shared level holding ~1.1x the mean visited set at load 3/4 (12-32 KB per warp),
@@ -161,6 +163,8 @@ int32_t plan_warp(dk_index* ix, SearchParams& P, LaunchPlan& L, int mode, double
   slots = std::min<uint32_t>(slots, ((budget - base) / 4) & ~31u);
   if (const uint32_t hl = env_u32("DK_HASH_LOG2", 0)) slots = 1u << std::min<uint32_t>(hl, 16);
   slots = std::max<uint32_t>(slots, 64);
+  // The rerank list needs 2 (L + F) slots; a second queue buffer would have taken as much.
+  if (strategy_reranks(P.strategy)) slots = std::max<uint32_t>(slots, align_up(2u * P.cap, 32));
   P.hash_slots = slots;
   P.hash_limit = slots * 3 / 4;
   // One global round trip per adjacency row for every mode: measured faster than one per
