@@ -785,6 +785,22 @@ __device__ __forceinline__ void score_lp_wide(const SearchParams& P, const float
       }
       mt[u] = __ldg(meta + rid[u]);
     }
+    // Two to four rows per subgroup per round: once the first round's loads are out, the later
+    // rounds' rows and (scale, norm) pairs are requested into L2, so those rounds find them on
+    // chip.  Measured: BF16 1M x 128 +8-11 %, FP8 2M x 384 +8-13 %; with eight rows per round
+    // (FP8 at 128 dimensions, where a hop's second round holds a few rows) it cost 1-7 %.
+    if constexpr (U > 1 && U <= 4) {
+      if (b0 == 0u && count > step) {
+        constexpr uint32_t lines = (row_bytes + 127u) / 128u;
+        const uint32_t total = (count - step) * (lines + 1u);
+        for (uint32_t e = sg * 8u + s; e < total; e += nsub * 8u) {
+          const uint32_t r = ids[step + e / (lines + 1u)], l = e % (lines + 1u);
+          const void* a = l < lines ? static_cast<const void*>(base + (size_t)r * row_bytes + l * 128u)
+                                    : static_cast<const void*>(meta + r);
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
+        }
+      }
+    }
     float acc[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) acc[u] = 0.0f;
