@@ -1041,6 +1041,89 @@ __device__ __forceinline__ void record_hint(const SearchParams& P, uint32_t cmps
   }
 }
 
+// Rerank order (inmem/full_precision.rs:357-404 sorts by the exact distance): ascending
+// distance, equal distances in queue order.  The reference's comparator calls a NaN equal to
+// everything, which leaves its place unspecified; here NaN distances sort after every number,
+// in queue order.  True when entry (a, ai) precedes entry (b, bi).
+__device__ __forceinline__ bool rerank_before(float a, uint32_t ai, float b, uint32_t bi) {
+  const bool an = a != a, bn = b != b;
+  if (an != bn) return bn;
+  if (an) return ai < bi;
+  return a < b || (a == b && ai < bi);
+}
+
+// The first k entries of a rerank list (ids `rid`, exact distances `rd`, `count` entries) in
+// rerank order, by one warp.  Ranking every entry against the whole list costs O(count * k)
+// dependent shared-memory reads per lane when the low-precision queue order differs from the
+// exact order (FP8 on 2M x 384 at L = 512: ~8 % of a search).  Instead: T = the k-th smallest
+// key of a 32-entry sample (at first the first 32 entries), so at least k keys are <= T and the
+// k smallest all are; the keys <= T are gathered one per lane, and each one's rank among them
+// is its rank in the whole list (every smaller key is <= T too).  More than 32 keys <= T: the
+// first 32 of them become the sample and T shrinks; after 8 rounds, or when T is NaN, or for
+// short lists, every entry is ranked against the list.  Returns min(count, k).
+__device__ __forceinline__ uint32_t warp_rerank_select(const uint32_t* rid, const float* rd,
+                                                       uint32_t count, uint32_t k,
+                                                       uint32_t* out_ids, float* out_d,
+                                                       uint32_t lane) {
+  if (count >= 64u && k >= 1u && k <= 32u) {
+    float sd = rd[lane];  // sample: one key per lane
+    uint32_t si = lane;
+    for (int round = 0; round < 8; ++round) {
+      uint32_t r = 0;
+      for (uint32_t m = 0; m < 32u; ++m)
+        r += rerank_before(__shfl_sync(kFull, sd, m), __shfl_sync(kFull, si, m), sd, si);
+      const uint32_t src = __ffs(__ballot_sync(kFull, r == k - 1u)) - 1u;
+      const float td = __shfl_sync(kFull, sd, src);
+      const uint32_t ti = __shfl_sync(kFull, si, src);
+      if (td != td) break;
+      uint32_t nc = 0;  // keys <= T gathered so far; lane t holds the t-th
+      float cd = 0.0f;
+      uint32_t ci = 0;
+      for (uint32_t t0 = 0; t0 < count && nc <= 32u; t0 += 32u) {
+        const uint32_t i = t0 + lane;
+        const float d = i < count ? rd[i] : 0.0f;
+        const uint32_t m = __ballot_sync(kFull, i < count && !rerank_before(td, ti, d, i));
+        if (m == 0u) continue;
+        // Lane nc + q takes the q-th set lane of m (as many as fit in 32).
+        uint32_t from = lane;
+        const bool take = lane >= nc && lane - nc < (uint32_t)__popc(m);
+        if (take) {
+          uint32_t mm = m;
+          for (uint32_t q = lane - nc; q > 0u; --q) mm &= mm - 1u;
+          from = __ffs(mm) - 1u;
+        }
+        const float gd = __shfl_sync(kFull, d, from);
+        const uint32_t gi = __shfl_sync(kFull, i, from);
+        if (take) {
+          cd = gd;
+          ci = gi;
+        }
+        nc += __popc(m);
+      }
+      if (nc > 32u) {  // too many keys <= T: the first 32 of them are the next sample
+        sd = cd;
+        si = ci;
+        continue;
+      }
+      uint32_t rank = 0;
+      for (uint32_t m = 0; m < nc; ++m)
+        rank += rerank_before(__shfl_sync(kFull, cd, m), __shfl_sync(kFull, ci, m), cd, ci);
+      if (lane < nc && rank < k) {
+        out_ids[rank] = rid[ci];
+        out_d[rank] = cd;
+      }
+      return k;
+    }
+  }
+  for (uint32_t i = lane; i < count; i += 32u) {
+    const float d = rd[i];
+    uint32_t r = 0;
+    for (uint32_t j = 0; j < count && r < k; ++j) r += rerank_before(rd[j], j, d, i);
+    if (r < k) { out_ids[r] = rid[i]; out_d[r] = d; }
+  }
+  return min(count, k);
+}
+
 // ========================================================================================
 // CTA-per-query kernel.
 // ========================================================================================
@@ -1163,13 +1246,8 @@ __device__ void cta_post_process(const SearchParams& P, const State& S, uint32_t
     __syncthreads();
     for (uint32_t i = tid; i < count; i += NT) {
       const float d = rd[i];
-      const bool dn = d != d;
       uint32_t r = 0;
-      for (uint32_t j = 0; j < count && r < P.k; ++j) {
-        const float dj = rd[j];
-        const bool jn = dj != dj;
-        r += dn ? (jn && j < i) : (!jn && (dj < d || (dj == d && j < i)));
-      }
+      for (uint32_t j = 0; j < count && r < P.k; ++j) r += rerank_before(rd[j], j, d, i);
       if (r < P.k) { out_ids[r] = rid[i]; out_d[r] = d; }
     }
     written = min(count, P.k);
@@ -1589,18 +1667,7 @@ __device__ void warp_post_process(const SearchParams& P, const State& S, const Q
     const uint32_t count = base;
     __syncwarp();
     warp_score<METRIC, kModeFP32, DIM, U>(P, S, rid, rd, count, lane);
-    for (uint32_t i = lane; i < count; i += 32u) {
-      const float d = rd[i];
-      const bool dn = d != d;
-      uint32_t r = 0;
-      for (uint32_t j = 0; j < count && r < k; ++j) {
-        const float dj = rd[j];
-        const bool jn = dj != dj;
-        r += dn ? (jn && j < i) : (!jn && (dj < d || (dj == d && j < i)));
-      }
-      if (r < k) { out_ids[r] = rid[i]; out_d[r] = d; }
-    }
-    written = min(count, k);
+    written = warp_rerank_select(rid, rd, count, k, out_ids, out_d, lane);
   }
   for (uint32_t j = written + lane; j < k; j += 32u) {
     out_ids[j] = DK_INVALID_ID;

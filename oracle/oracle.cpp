@@ -610,7 +610,8 @@ extern "C" void orc_paged_destroy(orc_paged* ps) { delete ps; }
 //
 // Rerank sorts with `sort_unstable_by` in the reference; this restatement uses a stable
 // sort (equal full-precision distances keep queue order), which is one of the orders the
-// reference may produce.
+// reference may produce.  The reference's comparator calls a NaN equal to everything, which
+// leaves a NaN's place unspecified; here NaN distances sort after every number, in queue order.
 extern "C" int32_t orc_search(const orc_index* ix, int32_t strategy, const float* query,
                               uint32_t k, uint32_t l, uint32_t beam_width, uint32_t* ids_out,
                               float* dists_out, orc_stats* stats) {
@@ -650,7 +651,8 @@ extern "C" int32_t orc_search(const orc_index* ix, int32_t strategy, const float
       rr.emplace_back(id, orc_distance(ix->metric, query, vec_row(ix, id), ix->dim));
     }
     std::stable_sort(rr.begin(), rr.end(), [](const auto& a, const auto& b) {
-      return a.second < b.second;
+      const bool an = std::isnan(a.second), bn = std::isnan(b.second);
+      return an != bn ? bn : (!an && a.second < b.second);
     });
     for (size_t i = 0; i < rr.size() && count < k; ++i, ++count) {
       ids_out[count] = rr[i].first;

@@ -166,6 +166,34 @@ def test_nan_vectors_are_scored_not_inserted(kernel):
                 orc.search(q, 10, 30, 1, O.STRATEGY_FULL_PRECISION))
 
 
+@pytest.mark.parametrize("nan_every", [0, 5, 1])
+def test_rerank_order_long_lists_and_nan_rows(nan_every, kernel):
+    """Hybrid rerank over lists of 50-300 entries.  A coarse PQ (4 chunks) leaves the queue far
+    from the exact order, so the warp kernel's top-k selection needs several sample rounds.
+    Rows with a NaN coordinate reach the rerank through their finite PQ codes and sort after
+    every number, in queue order (nan_every=1: nine rows in ten carry a NaN)."""
+    v, a, d, n = random_index(3000, 64, 24, seed=71, max_degree=31)
+    off, piv, codes = simple_pq(v, 4, seed=72)
+    q = queries_like(v[:n], 32, seed=73)
+    if nan_every == 5:
+        v[:n:5, 7] = np.nan
+    elif nan_every == 1:
+        v[:n][np.arange(n) % 10 != 3, 7] = np.nan
+    idx = DiskANNIndex(GpuProvider(v, a, d, n, Metric.L2, pq=PQData(off, piv, codes)))
+    orc = O.OracleIndex(v, a, d, n, O.METRIC_L2, off, piv, codes)
+    for k, l in [(10, 50), (10, 200), (32, 300), (1, 100), (40, 120)]:
+        gi, gd, gs = idx.search(Knn(k, l), Hybrid(), q)
+        oi, od, os_ = orc.search(q, k, l, 1, O.STRATEGY_HYBRID, threads=4)
+        np.testing.assert_array_equal(gi, oi)
+        nan = np.isnan(od)
+        np.testing.assert_array_equal(np.isnan(gd), nan)
+        np.testing.assert_array_equal(gd[~nan].view(np.uint32), od[~nan].view(np.uint32))
+        for key in ("cmps", "hops", "result_count"):
+            np.testing.assert_array_equal(gs[key], os_[key])
+        if nan_every == 1 and k >= 32:
+            assert nan.any()
+
+
 def test_k_equals_l_and_small_graph(kernel):
     v, a, d, n = random_index(50, 4, 6, seed=61, max_degree=6)
     q = queries_like(v[:n], 8, seed=62)
