@@ -57,7 +57,9 @@ enum dk_strategy {
   /* Hybrid-style strategies over low-precision copies of the vectors (no counterpart in the
    * reference): candidates are scored from BF16 rows, or from FP8-E4M3 rows with one FP32
    * scale per vector, accumulating in FP32; the queue is then re-ranked with exact FP32
-   * distances (the reference's Rerank, inmem/full_precision.rs:357-404). */
+   * distances (the reference's Rerank, inmem/full_precision.rs:357-404).
+   * Rerank order, every reranking strategy: ascending exact distance, ties in queue order, NaN
+   * distances (rows holding a NaN) after every number, in queue order. */
   DK_STRATEGY_BF16 = 3,
   DK_STRATEGY_FP8 = 4,
 };
