@@ -787,7 +787,7 @@ __device__ __forceinline__ void score_lp_wide(const SearchParams& P, const float
     }
     // Two to four rows per subgroup per round: once the first round's loads are out, the later
     // rounds' rows and (scale, norm) pairs are requested into L2, so those rounds find them on
-    // chip.  Measured: BF16 1M x 128 +8-11 %, FP8 2M x 384 +8-13 %; with eight rows per round
+    // chip.  Measured: BF16 1M x 128 +7-11 %, FP8 2M x 384 +8-12 %; with eight rows per round
     // (FP8 at 128 dimensions, where a hop's second round holds a few rows) it cost 1-7 %.
     if constexpr (U > 1 && U <= 4) {
       if (b0 == 0u && count > step) {
@@ -1055,7 +1055,7 @@ __device__ __forceinline__ bool rerank_before(float a, uint32_t ai, float b, uin
 // The first k entries of a rerank list (ids `rid`, exact distances `rd`, `count` entries) in
 // rerank order, by one warp.  Ranking every entry against the whole list costs O(count * k)
 // dependent shared-memory reads per lane when the low-precision queue order differs from the
-// exact order (FP8 on 2M x 384 at L = 512: ~8 % of a search).  Instead: T = the k-th smallest
+// exact order (FP8 on 2M x 384 at L = 512: ~4 % of a search).  Instead: T = the k-th smallest
 // key of a 32-entry sample (at first the first 32 entries), so at least k keys are <= T and the
 // k smallest all are; the keys <= T are gathered one per lane, and each one's rank among them
 // is its rank in the whole list (every smaller key is <= T too).  More than 32 keys <= T: the
