@@ -304,3 +304,25 @@ def test_oracle_paged_errors():
     for k in (0, 9):
         with pytest.raises(ValueError):
             ps.next_page(k)
+
+
+def test_oracle_rerank_sorts_nan_last():
+    """Hybrid rerank order in the oracle: ascending exact distance, NaN distances (rows with a
+    NaN coordinate, reachable through their finite PQ codes) after every number."""
+    from tests.helpers import random_index, simple_pq
+
+    v, a, d, n = random_index(600, 16, 12, seed=81, max_degree=12)
+    off, piv, codes = simple_pq(v, 4, seed=82)
+    v[:n][np.arange(n) % 3 != 0, 5] = np.nan
+    ix = O.OracleIndex(v, a, d, n, O.METRIC_L2, off, piv, codes)
+    q = np.nan_to_num(v[:8]) + 0.25
+    ids, dists, stats = ix.search(q, 40, 100, 1, O.STRATEGY_HYBRID)
+    saw_nan = False
+    for row, cnt in zip(dists, stats["result_count"]):
+        row = row[:cnt]
+        nan = np.isnan(row)
+        first = int(np.argmax(nan)) if nan.any() else len(row)
+        assert not nan[:first].any() and nan[first:].all()
+        assert (np.diff(row[:first]) >= 0).all()
+        saw_nan |= bool(nan.any())
+    assert saw_nan
